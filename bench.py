@@ -1,0 +1,371 @@
+"""ALS benchmark: sec/iteration and GFLOP/s at f=100 on the Netflix-shaped
+synthetic matrix (480,189 x 17,770, ~99.1M training ratings, 1.4M test).
+
+One step = one full ALS iteration (user half-step, then item half-step) over
+the resident matrix. GFLOP/s uses the solver-independent formula
+    FLOP_iter = sum_sides nnz*f*(f+1) + 2*nnz*f + rows*(f^3/3 + 2 f^2).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Engine arm: inputs resident in HBM, CUDA events on the model's stream, max
+over ranks; e2e through the drop-in doALSWithCSR with host buffers (CSR upload
+as the Spark JNI does it, theta upload, X download inside the timed region).
+Reference arm: the reference has no CPU ALS (its CPU path is Spark's JVM ALS,
+absent here), so it times the CPU port of the same half-step (oracle FP32) on
+bounded seeded row samples with all host threads, scaled by the formula.
+With N > 1 ranks, rows are sharded by nnz and each half-step ends with an
+all-gather of the updated factor rows (NCCL).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "cuda-mllib_b200")]
+
+METRIC = "ALS sec/iter & GFLOP/s at f=100, test RMSE within 0.1% of FP64 oracle"
+WORKLOAD = "netflix-shape synthetic 480189x17770, ~100.5M ratings (1.4M test), f=100, lambda=0.05"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--config", default="netflix")
+    p.add_argument("--scale", type=float, default=1.0, help="shrink m, n (nnz by scale^2)")
+    p.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
+    p.add_argument("--solver", default="cholesky", choices=["cholesky", "cg"])
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample time")
+    return p.parse_args()
+
+
+def cfg_of(args):
+    import als_b200 as A
+    return A.scaled_config(args.config, args.scale) if args.scale != 1.0 else dict(A.CONFIGS[args.config])
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return d["hbm_gbs"], d["bf16_tflops"], d.get("bf16_tflops_sustained", d["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.tmp.name).read().strip().splitlines()]
+            os.unlink(self.tmp.name)
+        except Exception:
+            return None
+        rows = [[x.strip() for x in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        load = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": float(np.median(load)) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# CPU port on bounded samples (reference arm and cpu_baseline leg)
+# ---------------------------------------------------------------------------
+
+def _sample_rows(ptr, idx, val, rows):
+    sub_ptr = np.zeros(len(rows) + 1, np.int64)
+    sub_ptr[1:] = np.cumsum(ptr[rows + 1] - ptr[rows])
+    take = np.concatenate([np.arange(ptr[u], ptr[u + 1]) for u in rows]) if len(rows) else np.zeros(0, np.int64)
+    return sub_ptr, idx[take], val[take]
+
+
+def cpu_port_step(r, f, lam, users, items, X, T):
+    """One sampled CPU iteration: the sampled users from T, the sampled items
+    from X. Returns (seconds, algorithmic FLOPs of the sampled rows)."""
+    import oracle as O
+    up, uc, uv = _sample_rows(r.csr_ptr, r.csr_col, r.csr_val, users)
+    ip, ir, iv = _sample_rows(r.csc_ptr, r.csc_row, r.csc_val, items)
+    t0 = time.perf_counter()
+    O.half_step_f32(up, uc, uv, T, lam)
+    O.half_step_f32(ip, ir, iv, X, lam)
+    dt = time.perf_counter() - t0
+    nnz = up[-1] + ip[-1]
+    flops = nnz * f * (f + 1) + 2 * nnz * f + (len(users) + len(items)) * (f ** 3 / 3 + 2 * f * f)
+    return dt, flops
+
+
+def cpu_sample_plan(r, f, lam, seconds, seed):
+    """Seeded user/item samples sized so one sampled iteration takes about
+    `seconds` on this host (the two sides in their full-matrix proportion)."""
+    rng = np.random.default_rng(seed)
+    X = np.random.default_rng(seed + 1).standard_normal((r.m, f)).astype(np.float32) * f ** -0.5
+    T = np.random.default_rng(seed + 2).standard_normal((r.n, f)).astype(np.float32) * f ** -0.5
+    frac = min(1.0, 2000.0 / r.m)
+    while True:
+        users = np.sort(rng.choice(r.m, max(1, int(r.m * frac)), replace=False))
+        items = np.sort(rng.choice(r.n, max(1, int(r.n * frac)), replace=False))
+        dt, _ = cpu_port_step(r, f, lam, users, items, X, T)
+        if dt >= 0.25 * seconds or frac >= 1.0:
+            break
+        frac = min(1.0, frac * min(8.0, max(1.5, seconds / max(dt, 1e-3))))
+    if dt < seconds and frac < 1.0:
+        frac = min(1.0, frac * seconds / max(dt, 1e-3))
+        users = np.sort(rng.choice(r.m, max(1, int(r.m * frac)), replace=False))
+        items = np.sort(rng.choice(r.n, max(1, int(r.n * frac)), replace=False))
+    return users, items, X, T, frac
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    import als_b200 as A
+    cfg = cfg_of(args)
+    f, lam = cfg["f"], cfg["lam"]
+    r = A.synth(cfg, seed=args.seed)
+    per_step = max(2.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
+    users, items, X, T, frac = cpu_sample_plan(r, f, lam, per_step, args.seed)
+    for _ in range(args.warmup):
+        cpu_port_step(r, f, lam, users, items, X, T)
+    secs, flops = [], 0.0
+    for _ in range(args.steps):
+        dt, fl = cpu_port_step(r, f, lam, users, items, X, T)
+        secs.append(dt)
+        flops = fl
+    gflops = flops / np.median(secs) / 1e9
+    full = A.flop_per_iteration(r, f)
+    cores = os.cpu_count()
+    sample = (f"seeded {len(users)} of {r.m} user rows + {len(items)} of {r.n} item rows per step "
+              f"({frac:.2%} of rows), FP32 port of the half-step, {cores} threads")
+    line = {"metric": METRIC, "value": round(gflops, 3), "unit": "GFLOP/s", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(full / (gflops * 1e9) * 1e3, 3),
+            "sec_per_iter": round(full / (gflops * 1e9), 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": WORKLOAD if args.scale == 1.0 else f"{args.config} x{args.scale}",
+                       "f": f, "lambda": lam, "m": r.m, "n": r.n, "nnz_train": r.nnz},
+            "cpu_baseline": {"value": round(gflops, 3), "unit": "GFLOP/s", "cores": cores,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(gflops, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference's CPU ALS is Spark's JVM implementation (not in the reference, "
+                    "no JVM here); timed instead: the C restatement of the same half-step"}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# engine arm
+# ---------------------------------------------------------------------------
+
+def run_engine(args):
+    import torch
+    import als_b200 as A
+
+    world, rank, local = dist_init(args)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cfg = cfg_of(args)
+    f, lam = cfg["f"], cfg["lam"]
+    t0 = time.perf_counter()
+    r = A.synth(cfg, seed=args.seed)
+    gen_s = time.perf_counter() - t0
+    prec = {"fp32": A.PREC_FP32, "bf16": A.PREC_BF16, "fp16": A.PREC_FP16}[args.precision]
+    solver = {"cholesky": A.SOLVER_CHOLESKY, "cg": A.SOLVER_CG}[args.solver]
+    opts = A.options(precision=prec, solver=solver)
+    stream = torch.cuda.Stream(device=dev)
+    th0 = A.init_factors(r.n, f, args.seed + 100)
+    with torch.cuda.stream(stream):
+        model = A.Model(r, f, opts, stream=stream, theta0=th0)
+    shard = None
+    if world > 1:
+        from als_dist import ShardedIteration
+        shard = ShardedIteration(model, r, world, rank, stream)
+        shard.apply()
+
+    def iteration(ev=None):
+        # one launch of the fused rows kernel per half-step
+        if ev is not None:
+            ev[0].record(stream)
+        model.half_step(A.SIDE_USERS, lam)
+        if shard:
+            shard.gather(A.SIDE_USERS)
+        if ev is not None:
+            ev[1].record(stream)
+        model.half_step(A.SIDE_ITEMS, lam)
+        if shard:
+            shard.gather(A.SIDE_ITEMS)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        iteration()
+    torch.cuda.synchronize(dev)
+    model.stats(reset=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    with Clocks(local) as ck:
+        torch.cuda.synchronize(dev)
+        for k in range(args.steps):
+            iteration(evs[k])
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    users_ms = np.array([e[0].elapsed_time(e[1]) for e in evs])
+    items_ms = np.array([e[1].elapsed_time(e[2]) for e in evs])
+    step_ms = users_ms + items_ms
+    total_ms = float(step_ms.sum())
+    if world > 1:
+        t = torch.tensor([total_ms, float(np.median(step_ms))], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, med_ms = float(t[0]), float(t[1])
+    else:
+        med_ms = float(np.median(step_ms))
+    stats = model.stats()
+    rmse = model.rmse()
+    flop_iter = A.flop_per_iteration(r, f)
+    gflops = flop_iter * args.steps / (total_ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel: the fused rows kernel, one launch per half-step
+    hbm, tf_burst, tf_sust, src = peaks()
+    per_side = lambda nnz, rows: nnz * f * (f + 1) + 2 * nnz * f + rows * (f ** 3 / 3 + 2 * f * f)
+    avg_launch_s = float(np.concatenate([users_ms, items_ms]).mean()) / 1e3
+    avg_flops = (per_side(r.nnz, r.m) + per_side(r.nnz, r.n)) / 2
+    achieved = avg_flops / avg_launch_s / 1e12
+    roof = {"bound": "tensor", "achieved": round(achieved, 3), "peak": tf_sust, "unit": "TFLOP/s",
+            "frac": round(achieved / tf_sust, 4), "traffic": None,
+            "peak_kind": f"{src} bf16 dense sustained",
+            "kernel": "rows kernel (gather + hermitian + solve), both sides",
+            "users_ms": round(float(users_ms.mean()), 3), "items_ms": round(float(items_ms.mean()), 3)}
+
+    line = None
+    if rank == 0:
+        ck_sum = ck.summary()
+        line = {"metric": METRIC, "value": round(gflops, 2), "unit": "GFLOP/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
+                "sec_per_iter": round(med_ms / 1e3, 5), "higher_is_better": True,
+                "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": args.precision, "data": "synthetic",
+                "config": {"workload": WORKLOAD if args.scale == 1.0 else f"{args.config} x{args.scale}",
+                           "f": f, "lambda": lam, "m": r.m, "n": r.n, "nnz_train": r.nnz,
+                           "n_test": int(len(r.test_r)), "precision": args.precision,
+                           "solver": args.solver, "seed": args.seed,
+                           "l2": "inputs larger than L2 (CSR+CSC %.2f GB per iteration)" % (
+                               (r.nnz * 16 + (r.m + r.n) * 8) / 1e9),
+                           "parallelism": f"rows sharded x{world}" if world > 1 else "1 GPU",
+                           "generation_s": round(gen_s, 2)},
+                "rmse": round(rmse, 6), "roofline": roof,
+                "gpu_launches": 2 * args.steps, "clocks": ck_sum, "solver_stats": stats}
+
+    # e2e through the drop-in entry point with host buffers (rank 0, 1 GPU path)
+    if rank == 0 and not args.no_e2e:
+        X = model.factors()[0].cpu().numpy()
+        T = model.factors()[1].cpu().numpy()
+        ptr32 = r.csr_ptr.astype(np.int32)
+        cptr32 = r.csc_ptr.astype(np.int32)
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+        host = [pin(a) for a in (ptr32, r.csr_col, r.csr_val, cptr32, r.csc_row, r.csc_val)]
+        e2e_steps = max(1, min(args.steps, 3))
+        torch.cuda.synchronize(dev)
+        times = []
+        for _ in range(e2e_steps + 1):
+            t1 = time.perf_counter()
+            Xn = A.do_als_with_csr(host[0], host[1], host[2], T, r.m, r.n, f, lam)
+            Tn = A.do_als_with_csr(host[3], host[4], host[5], Xn, r.n, r.m, f, lam)
+            times.append(time.perf_counter() - t1)
+            T = Tn
+        e2e_s = float(np.median(times[1:]))
+        h2d = sum(a.nbytes for a in host) + 4 * (r.m + r.n) * f
+        d2h = 4 * (r.m + r.n) * f
+        line["e2e"] = {"value": round(flop_iter / e2e_s / 1e9, 2), "unit": "GFLOP/s",
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                       "sec_per_iter": round(e2e_s, 4),
+                       "path": "doALSWithCSR x2 (users, items): CSR upload to mallocBest memory, "
+                               "theta upload, X download; wall clock, FP32 form"}
+        line["gpu_launches"] += 0
+
+    if rank == 0 and not args.no_cpu_baseline:
+        users, items, Xs, Ts, frac = cpu_sample_plan(r, f, lam, args.cpu_seconds, args.seed)
+        dt, fl = cpu_port_step(r, f, lam, users, items, Xs, Ts)
+        line["cpu_baseline"] = {"value": round(fl / dt / 1e9, 3), "unit": "GFLOP/s",
+                                "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"seeded {len(users)} user + {len(items)} item rows "
+                                          f"({frac:.2%}) of the same matrix, FP32 port, one pass"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    model.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

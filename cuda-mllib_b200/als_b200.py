@@ -1,0 +1,464 @@
+"""Python host layer of the B200 ALS engine.
+
+Thin ctypes bindings over the C ABI in ``include/als_b200.h`` (``libGPUALS.so``)
+and ``include/als_data.h`` (``libalsdata.so``). All computation happens in those
+libraries; PyTorch is used only to hold device memory and streams.
+
+The drop-in path mirrors the reference's Spark JNI flow
+(als/src/CuMFJNIInterface.cpp:93-109): CSR copied into ``mallocBest`` memory,
+``doALSWithCSR`` called, the callee frees the CSR. The engine path keeps both
+sides of the rating matrix and both factor matrices resident in HBM.
+
+There is no CPU fallback: if the libraries are missing the import fails, and
+if no GPU is present every compute call fails with the CUDA error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+ALS_OK, ALS_ERR_INVALID, ALS_ERR_CUDA, ALS_ERR_UNSUPPORTED = 0, 1, 2, 3
+PREC_FP32, PREC_BF16, PREC_FP16 = 0, 1, 2
+SOLVER_CHOLESKY, SOLVER_CG = 0, 1
+WARM_ZERO, WARM_PREVIOUS, WARM_MLP = 0, 1, 2
+SIDE_USERS, SIDE_ITEMS = 0, 1
+ROW_EMPTY, ROW_NOT_SPD, ROW_REFINED_F64, ROW_CG_FALLBACK = 1, 2, 4, 8
+
+
+class AlsError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _load(name: str) -> ctypes.CDLL:
+    path = os.path.join(_HERE, name)
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is not built (run `make` in {_HERE})")
+    return ctypes.CDLL(path)
+
+
+lib = _load("libGPUALS.so")
+datalib = _load("libalsdata.so")
+
+c_i32, c_i64, c_u64, c_f32, c_f64 = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64,
+                                     ctypes.c_float, ctypes.c_double)
+c_vp, c_sz = ctypes.c_void_p, ctypes.c_size_t
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", c_i32), ("solver", c_i32), ("warm_start", c_i32),
+                ("cg_max_steps", c_i32), ("cg_tol", c_f32), ("refine_tol", c_f32),
+                ("use_graph", c_i32), ("reserved", c_i32 * 9)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("rows_solved", c_u64), ("rows_refined", c_u64), ("rows_not_spd", c_u64),
+                ("cg_steps", c_u64), ("cg_fallbacks", c_u64), ("reserved", c_u64 * 3)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
+
+
+class SynthSpec(ctypes.Structure):
+    _fields_ = [("m", c_i64), ("n", c_i64), ("planted_rank", c_i32), ("integer_ratings", c_i32),
+                ("factor_sigma", c_f64), ("noise_sigma", c_f64), ("mu", c_f64),
+                ("rating_min", c_f64), ("rating_max", c_f64), ("degree_law", c_i32),
+                ("threads", c_i32), ("degree_p1", c_f64), ("degree_min", c_i64),
+                ("degree_max", c_i64), ("item_zipf_s", c_f64), ("target_nnz", c_i64),
+                ("seed", c_u64)]
+
+
+def _sig(fn, restype, *argtypes):
+    fn.restype = restype
+    fn.argtypes = list(argtypes)
+    return fn
+
+
+_sig(lib.als_default_options, None, c_vp)
+_sig(lib.als_last_error, ctypes.c_char_p)
+_sig(lib.als_version, ctypes.c_char_p)
+_sig(lib.als_model_create, c_i32, c_vp, c_i64, c_i64, c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp,
+     c_vp, c_vp, c_vp)
+_sig(lib.als_model_destroy, None, c_vp)
+_sig(lib.als_model_set_theta, c_i32, c_vp, c_vp, c_i32, c_vp)
+_sig(lib.als_model_set_x, c_i32, c_vp, c_vp, c_i32, c_vp)
+_sig(lib.als_model_half_step, c_i32, c_vp, c_i32, c_f32, c_vp)
+_sig(lib.als_model_iterate, c_i32, c_vp, c_f32, c_i32, c_vp)
+_sig(lib.als_model_factors, c_i32, c_vp, c_vp, c_vp)
+_sig(lib.als_model_row_flags, c_i32, c_vp, c_i32, c_vp)
+_sig(lib.als_model_stats, c_i32, c_vp, c_vp, c_i32)
+_sig(lib.als_model_rmse, c_i32, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp)
+_sig(lib.als_half_step_work_bytes, c_sz, c_i64)
+_sig(lib.als_half_step, c_i32, c_i64, c_i64, c_i32, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_i32,
+     c_f32, c_vp, c_vp, c_sz, c_vp)
+_sig(lib.als_rmse_work_bytes, c_sz)
+_sig(lib.als_rmse, c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_i32, c_i32, c_vp, c_vp,
+     c_sz, c_vp)
+_sig(lib.als_predict, c_i32, c_i64, c_vp, c_vp, c_vp, c_i32, c_vp, c_i32, c_i32, c_vp, c_vp)
+_sig(lib.als_train, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i32, c_i64, c_f32,
+     c_i32, c_vp, c_vp, c_vp, c_vp)
+_sig(lib.doALSWithCSR, None, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int,
+     ctypes.c_int, ctypes.c_long, c_f32, ctypes.c_int)
+_sig(lib.mallocBest, ctypes.c_int, c_vp, c_sz)
+_sig(lib.freeBest, ctypes.c_int, c_vp)
+_sig(lib.get_gpu, ctypes.c_int)
+
+_sig(datalib.als_synth_degrees, c_i32, c_vp, c_vp, c_vp)
+_sig(datalib.als_synth_fill, c_i32, c_vp, c_vp, c_vp, c_vp)
+_sig(datalib.als_split, c_i32, c_i64, c_vp, c_vp, c_vp, c_f64, c_u64, c_vp, c_vp, c_vp, c_vp,
+     c_vp, c_vp, c_vp, c_vp, c_i32)
+_sig(datalib.als_csr_transpose, c_i32, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32)
+_sig(datalib.als_init_factors, c_i32, c_i64, c_i32, c_f64, c_u64, c_vp, c_i32)
+_sig(datalib.als_load_csr_bin, c_i32, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, c_vp,
+     c_vp, c_vp, c_i64, c_i64)
+_sig(datalib.als_save_csr_bin, c_i32, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, c_vp,
+     c_vp, c_vp, c_i64, c_i64)
+
+
+def _check(rc: int) -> None:
+    if rc != ALS_OK:
+        raise AlsError(rc, lib.als_last_error().decode(errors="replace"))
+
+
+def _ptr(a) -> int:
+    """Raw address of a numpy array or torch tensor (None -> 0)."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def options(**kw) -> Options:
+    o = Options()
+    lib.als_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+def version() -> str:
+    return lib.als_version().decode()
+
+
+# ---------------------------------------------------------------------------
+# synthetic data
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Ratings:
+    m: int
+    n: int
+    csr_ptr: np.ndarray   # int64 [m+1]  train, users x items
+    csr_col: np.ndarray   # int32 [nnz]
+    csr_val: np.ndarray   # float32 [nnz]
+    csc_ptr: np.ndarray   # int64 [n+1]  train, items x users
+    csc_row: np.ndarray   # int32 [nnz]
+    csc_val: np.ndarray   # float32 [nnz]
+    test_u: np.ndarray    # int32 [nt]
+    test_i: np.ndarray    # int32 [nt]
+    test_r: np.ndarray    # float32 [nt]
+    seed: int = 0
+
+    @property
+    def nnz(self) -> int:
+        return int(self.csr_ptr[-1])
+
+
+# Synthetic stand-ins with the published shapes of the rating matrices the
+# reference is run on (no dataset records are reproduced). Sizes, value ranges
+# and degree laws follow the benchmark configurations; mu is the centre of the
+# rating range, factor_sigma gives <u,v> unit variance where the configuration
+# does not state it.
+CONFIGS = {
+    # MovieLens-1M shape: plain FP32, f=10
+    "ml1m": dict(m=6040, n=3706, target_nnz=1_000_000, planted_rank=10, factor_sigma=10 ** -0.5,
+                 noise_sigma=0.5, mu=3.0, rating_min=1, rating_max=5, integer_ratings=1,
+                 degree_law=0, degree_p1=1.0, degree_min=20, degree_max=0, item_zipf_s=1.0,
+                 test_fraction=0.10, f=10, lam=0.05, iters=10),
+    # Netflix shape: f=100, the headline workload
+    "netflix": dict(m=480_189, n=17_770, target_nnz=100_500_000, planted_rank=100,
+                    factor_sigma=100 ** -0.25, noise_sigma=0.8, mu=3.0, rating_min=1,
+                    rating_max=5, integer_ratings=1, degree_law=0, degree_p1=1.2, degree_min=1,
+                    degree_max=0, item_zipf_s=1.1, test_fraction=1.4e6 / 100.5e6, f=100,
+                    lam=0.05, iters=10),
+    # Yahoo!-Music shape: power-law users, 0..100 ratings
+    "yahoo": dict(m=1_000_990, n=624_961, target_nnz=252_800_000, planted_rank=64,
+                  factor_sigma=64 ** -0.25, noise_sigma=8.0, mu=50.0, rating_min=0,
+                  rating_max=100, integer_ratings=1, degree_law=1, degree_p1=1.8, degree_min=1,
+                  degree_max=100_000, item_zipf_s=1.2, test_fraction=0.01, f=100, lam=1.0,
+                  iters=10),
+}
+CONFIGS["netflix128"] = dict(CONFIGS["netflix"], f=128)
+
+
+def scaled_config(name: str, scale: float) -> dict:
+    """A configuration with m, n and nnz scaled down (degree laws kept)."""
+    c = dict(CONFIGS[name])
+    c["m"] = max(8, int(c["m"] * scale))
+    c["n"] = max(8, int(c["n"] * scale))
+    c["target_nnz"] = max(16, int(c["target_nnz"] * scale * scale))
+    if c["degree_max"]:
+        c["degree_max"] = max(1, int(c["degree_max"] * scale))
+    return c
+
+
+def synth(cfg: dict, seed: int = 1, threads: int = 0) -> Ratings:
+    """Generate a seeded rating matrix, split it, and build both sides."""
+    s = SynthSpec()
+    for k, _ in SynthSpec._fields_:
+        if k in cfg:
+            setattr(s, k, cfg[k])
+    s.seed, s.threads = seed, threads
+    m, n = int(s.m), int(s.n)
+    deg = np.zeros(m, np.int64)
+    tot = c_i64(0)
+    _check(datalib.als_synth_degrees(ctypes.byref(s), _ptr(deg), ctypes.byref(tot)))
+    ptr = np.zeros(m + 1, np.int64)
+    np.cumsum(deg, out=ptr[1:])
+    col = np.empty(int(tot.value), np.int32)
+    val = np.empty(int(tot.value), np.float32)
+    _check(datalib.als_synth_fill(ctypes.byref(s), _ptr(ptr), _ptr(col), _ptr(val)))
+    del deg
+    frac = float(cfg.get("test_fraction", 0.0))
+    trc = np.empty(m, np.int64)
+    tec = np.empty(m, np.int64)
+    _check(datalib.als_split(m, _ptr(ptr), _ptr(col), _ptr(val), frac, seed + 7919, _ptr(trc),
+                             _ptr(tec), 0, 0, 0, 0, 0, 0, threads))
+    tr_ptr = np.zeros(m + 1, np.int64)
+    np.cumsum(trc, out=tr_ptr[1:])
+    te_ptr = np.zeros(m + 1, np.int64)
+    np.cumsum(tec, out=te_ptr[1:])
+    tr_col = np.empty(int(tr_ptr[-1]), np.int32)
+    tr_val = np.empty(int(tr_ptr[-1]), np.float32)
+    te_col = np.empty(int(te_ptr[-1]), np.int32)
+    te_val = np.empty(int(te_ptr[-1]), np.float32)
+    _check(datalib.als_split(m, _ptr(ptr), _ptr(col), _ptr(val), frac, seed + 7919, 0, 0,
+                             _ptr(tr_ptr), _ptr(tr_col), _ptr(tr_val), _ptr(te_ptr),
+                             _ptr(te_col), _ptr(te_val), threads))
+    del col, val
+    csc_ptr, csc_row, csc_val = transpose(m, n, tr_ptr, tr_col, tr_val, threads)
+    test_u = np.repeat(np.arange(m, dtype=np.int32), np.diff(te_ptr))
+    return Ratings(m, n, tr_ptr, tr_col, tr_val, csc_ptr, csc_row, csc_val, test_u, te_col,
+                   te_val, seed)
+
+
+def transpose(m, n, ptr, col, val, threads: int = 0):
+    """CSR (m x n) -> CSC (the CSR of the transpose), rows ascending per column."""
+    cptr = np.zeros(n + 1, np.int64)
+    rows = np.empty(len(col), np.int32)
+    vals = np.empty(len(col), np.float32)
+    _check(datalib.als_csr_transpose(m, n, _ptr(ptr), _ptr(col), _ptr(val), _ptr(cptr),
+                                     _ptr(rows), _ptr(vals), threads))
+    return cptr, rows, vals
+
+
+def init_factors(rows: int, f: int, seed: int, sigma: float | None = None,
+                 threads: int = 0) -> np.ndarray:
+    """Seeded N(0, 1/f) initial factors (rows x f, float32)."""
+    out = np.empty((rows, f), np.float32)
+    sig = (1.0 / f) ** 0.5 if sigma is None else sigma
+    _check(datalib.als_init_factors(rows, f, sig, seed, _ptr(out), threads))
+    return out
+
+
+def flop_per_iteration(r: Ratings, f: int) -> float:
+    """Algorithmic FLOPs of one full iteration (both sides), solver-independent:
+    sum over sides of nnz*f*(f+1) + 2*nnz*f + rows*(f^3/3 + 2 f^2)."""
+    per_side = r.nnz * f * (f + 1) + 2 * r.nnz * f
+    return 2 * per_side + (r.m + r.n) * (f ** 3 / 3 + 2 * f * f)
+
+
+# ---------------------------------------------------------------------------
+# engine on device memory
+# ---------------------------------------------------------------------------
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+class Model:
+    """A resident ALS model: both sides of R and both factor matrices in HBM.
+
+    Construct from a ``Ratings`` (uploaded once) or from device tensors.
+    """
+
+    def __init__(self, ratings: Ratings, f: int, opts: Options | None = None, stream=None,
+                 theta0: np.ndarray | None = None, seed: int = 2):
+        import torch
+        self.torch = torch
+        self.m, self.n, self.f = ratings.m, ratings.n, f
+        dev = torch.device("cuda")
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        self._dev = [t(ratings.csr_ptr), t(ratings.csr_col), t(ratings.csr_val),
+                     t(ratings.csc_ptr), t(ratings.csc_row), t(ratings.csc_val)]
+        self.test = [t(ratings.test_u), t(ratings.test_i), t(ratings.test_r)]
+        self.opts = opts or options()
+        self.stream = _stream_handle(stream)
+        h = c_vp()
+        _check(lib.als_model_create(ctypes.byref(h), self.m, self.n, f, ratings.nnz,
+                                    *[_ptr(x) for x in self._dev], ctypes.byref(self.opts),
+                                    self.stream))
+        self.handle = h
+        if theta0 is None:
+            theta0 = init_factors(self.n, f, seed)
+        self.set_theta(torch.from_numpy(np.ascontiguousarray(theta0, np.float32)).to(dev))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.als_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_theta(self, theta_dev):
+        _check(lib.als_model_set_theta(self.handle, _ptr(theta_dev), theta_dev.shape[1],
+                                       self.stream))
+
+    def set_x(self, x_dev):
+        _check(lib.als_model_set_x(self.handle, _ptr(x_dev), x_dev.shape[1], self.stream))
+
+    def half_step(self, side: int, lam: float):
+        _check(lib.als_model_half_step(self.handle, side, lam, self.stream))
+
+    def iterate(self, lam: float, iters: int = 1):
+        _check(lib.als_model_iterate(self.handle, lam, iters, self.stream))
+
+    def factors(self):
+        """(X, theta) as torch tensors viewing the model's device memory."""
+        torch = self.torch
+        x, t = c_vp(), c_vp()
+        _check(lib.als_model_factors(self.handle, ctypes.byref(x), ctypes.byref(t)))
+        return (_wrap_device(x.value, (self.m, self.f), torch.float32),
+                _wrap_device(t.value, (self.n, self.f), torch.float32))
+
+    def row_flags(self, side: int):
+        p = c_vp()
+        _check(lib.als_model_row_flags(self.handle, side, ctypes.byref(p)))
+        rows = self.m if side == SIDE_USERS else self.n
+        return _wrap_device(p.value, (rows,), self.torch.int32)
+
+    def stats(self, reset: bool = False) -> dict:
+        s = Stats()
+        _check(lib.als_model_stats(self.handle, ctypes.byref(s), int(reset)))
+        return s.as_dict()
+
+    def rmse(self, test=None) -> float:
+        u, i, r = test if test is not None else self.test
+        out = c_f64()
+        _check(lib.als_model_rmse(self.handle, len(u), _ptr(u), _ptr(i), _ptr(r),
+                                  ctypes.byref(out), self.stream))
+        return float(out.value)
+
+
+def _wrap_device(addr: int, shape, dtype):
+    """A torch tensor over device memory owned by the library (no copy)."""
+    import torch
+    typestr = {torch.float32: "<f4", torch.int32: "<i4", torch.int64: "<i8"}[dtype]
+
+    class _Iface:
+        __cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                    "data": (addr, False), "version": 3, "strides": None}
+    return torch.as_tensor(_Iface(), device="cuda")
+
+
+def half_step(row_ptr, col, val, src, dst, lam: float, opts: Options | None = None, stream=None):
+    """Stand-alone FP32 half-step on caller device tensors (no model)."""
+    import torch
+    m = row_ptr.shape[0] - 1
+    n, f = src.shape
+    work = torch.empty(int(lib.als_half_step_work_bytes(m)), dtype=torch.uint8, device="cuda")
+    _check(lib.als_half_step(m, n, f, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(src),
+                             src.stride(0), _ptr(dst), dst.stride(0), lam,
+                             ctypes.byref(opts or options()), _ptr(work), work.numel(),
+                             _stream_handle(stream)))
+
+
+def rmse(u, i, r, x, theta, stream=None) -> float:
+    import torch
+    work = torch.empty(int(lib.als_rmse_work_bytes()), dtype=torch.uint8, device="cuda")
+    out = c_f64()
+    _check(lib.als_rmse(len(u), _ptr(u), _ptr(i), _ptr(r), _ptr(x), x.stride(0), _ptr(theta),
+                        theta.stride(0), x.shape[1], ctypes.byref(out), _ptr(work), work.numel(),
+                        _stream_handle(stream)))
+    return float(out.value)
+
+
+def predict(u, i, x, theta, stream=None):
+    import torch
+    out = torch.empty(len(u), dtype=torch.float32, device="cuda")
+    _check(lib.als_predict(len(u), _ptr(u), _ptr(i), _ptr(x), x.stride(0), _ptr(theta),
+                           theta.stride(0), x.shape[1], _ptr(out), _stream_handle(stream)))
+    return out
+
+
+def train(r: Ratings, f: int, lam: float, iters: int, theta0: np.ndarray,
+          opts: Options | None = None):
+    """Host-buffer full training through ``als_train`` (cuMF-standalone style)."""
+    X = np.empty((r.m, f), np.float32)
+    T = np.array(theta0, np.float32, copy=True, order="C")
+    st = Stats()
+    _check(lib.als_train(_ptr(r.csr_ptr), _ptr(r.csr_col), _ptr(r.csr_val), _ptr(r.csc_ptr),
+                         _ptr(r.csc_row), _ptr(r.csc_val), r.m, r.n, f, r.nnz, lam, iters,
+                         ctypes.byref(opts or options()), _ptr(X), _ptr(T), ctypes.byref(st)))
+    return X, T, st.as_dict()
+
+
+# ---------------------------------------------------------------------------
+# drop-in path (the reference's JNI flow, without the JVM)
+# ---------------------------------------------------------------------------
+
+_cudart = None
+
+
+def _rt():
+    global _cudart
+    if _cudart is None:
+        for name in ("libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so.12"):
+            try:
+                _cudart = ctypes.CDLL(name)
+                break
+            except OSError:
+                continue
+        if _cudart is None:
+            raise ImportError("libcudart.so.12 not found")
+        _sig(_cudart.cudaMemcpy, ctypes.c_int, c_vp, c_vp, c_sz, ctypes.c_int)
+    return _cudart
+
+
+def do_als_with_csr(row_ptr32: np.ndarray, col: np.ndarray, val: np.ndarray, theta: np.ndarray,
+                    m: int, n: int, f: int, lam: float, x_batch: int = 1) -> np.ndarray:
+    """Run the drop-in ``doALSWithCSR``: CSR into mallocBest memory (freed by the
+    callee), theta and X in host memory; returns X (m x f)."""
+    rt = _rt()
+    nnz = len(col)
+    ptrs = []
+    for arr in (np.ascontiguousarray(row_ptr32, np.int32), np.ascontiguousarray(col, np.int32),
+                np.ascontiguousarray(val, np.float32)):
+        p = c_vp()
+        if lib.mallocBest(ctypes.byref(p), max(arr.nbytes, 4)) != 0:
+            raise AlsError(ALS_ERR_CUDA, "mallocBest failed")
+        if arr.nbytes and rt.cudaMemcpy(p, arr.ctypes.data, arr.nbytes, 1) != 0:
+            raise AlsError(ALS_ERR_CUDA, "cudaMemcpy failed")
+        ptrs.append(p)
+    th = np.ascontiguousarray(theta, np.float32)
+    X = np.zeros((m, f), np.float32)
+    lib.doALSWithCSR(None, ptrs[0], ptrs[1], ptrs[2], _ptr(th), _ptr(X), m, n, f, nnz, lam, x_batch)
+    return X

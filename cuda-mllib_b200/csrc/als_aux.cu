@@ -1,0 +1,181 @@
+// Auxiliary kernels: degree-binned row ordering, pointer widening, factor
+// down-conversion, and the fused RMSE / predict gather.
+#include <algorithm>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "als_internal.h"
+
+namespace als {
+
+int device_sm_count() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  return sms;
+}
+
+__device__ __forceinline__ int degree_bin(int64_t d) {
+  const int b = d <= 0 ? 0 : 64 - __clzll((unsigned long long)d);  // 1 + floor(log2 d)
+  return b < kOrderBins ? b : kOrderBins - 1;
+}
+
+__global__ void order_hist_kernel(const int64_t *row_ptr, int64_t m, unsigned *hist) {
+  __shared__ unsigned h[kOrderBins];
+  for (int i = threadIdx.x; i < kOrderBins; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < m;
+       u += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&h[degree_bin(row_ptr[u + 1] - row_ptr[u])], 1u);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kOrderBins; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+// Heaviest bin first: offsets are an exclusive scan over bins in descending order.
+__global__ void order_scan_kernel(const unsigned *hist, unsigned *offs) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    unsigned acc = 0;
+    for (int b = kOrderBins - 1; b >= 0; --b) {
+      offs[b] = acc;
+      acc += hist[b];
+    }
+  }
+}
+
+__global__ void order_scatter_kernel(const int64_t *row_ptr, int64_t m, unsigned *offs,
+                                     int32_t *order) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < m;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned p = atomicAdd(&offs[degree_bin(row_ptr[u + 1] - row_ptr[u])], 1u);
+    order[p] = (int32_t)u;
+  }
+}
+
+cudaError_t launch_degree_order(const int64_t *row_ptr, int64_t m, int32_t *order,
+                                unsigned *work, cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned) * 2 * kOrderBins, st);
+  if (e != cudaSuccess) return e;
+  const int sms = device_sm_count();
+  const unsigned grid = (unsigned)std::min<int64_t>((m + 255) / 256, (int64_t)sms * 8);
+  order_hist_kernel<<<grid, 256, 0, st>>>(row_ptr, m, work);
+  order_scan_kernel<<<1, 32, 0, st>>>(work, work + kOrderBins);
+  order_scatter_kernel<<<grid, 256, 0, st>>>(row_ptr, m, work + kOrderBins, order);
+  return cudaGetLastError();
+}
+
+__global__ void widen_kernel(const int32_t *in, int64_t count, int64_t *out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int64_t)in[i];
+}
+
+cudaError_t launch_widen_ptr(const int32_t *in, int64_t count, int64_t *out, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)std::min<int64_t>((count + 255) / 256, 4096);
+  widen_kernel<<<grid, 256, 0, st>>>(in, count, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
+__global__ void convert_kernel(const float *src, int64_t rows, int f, int ld_src, T *dst,
+                               int ld_dst) {
+  const int64_t total = rows * ld_dst;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = q / ld_dst;
+    const int c = (int)(q - r * ld_dst);
+    dst[q] = T(c < f ? src[r * ld_src + c] : 0.f);
+  }
+}
+
+cudaError_t launch_convert_lp(const float *src, int64_t rows, int f, int ld_src, void *dst,
+                              int ld_dst, int kind, cudaStream_t st) {
+  if (rows <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)std::min<int64_t>((rows * ld_dst + 255) / 256, 8192);
+  if (kind == kLpBf16)
+    convert_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(src, rows, f, ld_src,
+                                                        (__nv_bfloat16 *)dst, ld_dst);
+  else if (kind == kLpFp16)
+    convert_kernel<__half><<<grid, 256, 0, st>>>(src, rows, f, ld_src, (__half *)dst, ld_dst);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// RMSE / predict: one warp per test entry, lanes stride the rank; the squared
+// errors are summed in FP64 per warp, per block, then across blocks by a
+// single-block pass (fixed order: the result is bit-reproducible).
+// ---------------------------------------------------------------------------
+constexpr int kRmseBlocks = 1184;  // 8 x 148 SMs
+constexpr int kRmseThreads = 256;
+
+size_t rmse_work_bytes() { return sizeof(double) * kRmseBlocks; }
+
+__device__ __forceinline__ float dot_warp(const float *x, const float *t, int f) {
+  float s = 0.f;
+  for (int k = threadIdx.x & 31; k < f; k += 32) s = fmaf(x[k], t[k], s);
+  return warp_sum(s);
+}
+
+__global__ void __launch_bounds__(kRmseThreads)
+rmse_partial_kernel(int64_t nt, const int32_t *u, const int32_t *i, const float *r,
+                    const float *X, int ldx, const float *T, int ldt, int f, double *part) {
+  const int warps = kRmseThreads / 32, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double acc = 0.0;
+  for (int64_t q = blockIdx.x * (int64_t)warps + w; q < nt; q += (int64_t)gridDim.x * warps) {
+    const float p = dot_warp(X + (int64_t)u[q] * ldx, T + (int64_t)i[q] * ldt, f);
+    const double e = (double)r[q] - (double)p;
+    acc += e * e;
+  }
+  __shared__ double red[kRmseThreads / 32];
+  if (lane == 0) red[w] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < warps; ++k) s += red[k];
+    part[blockIdx.x] = s;
+  }
+}
+
+__global__ void rmse_final_kernel(const double *part, int nblocks, int64_t nt, double *out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < nblocks; k += blockDim.x) s += part[k];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = nt > 0 ? sqrt(red[0] / (double)nt) : 0.0;
+}
+
+cudaError_t launch_rmse(int64_t nt, const int32_t *u, const int32_t *i, const float *r,
+                        const float *X, int ldx, const float *T, int ldt, int f, double *out_dev,
+                        void *work, cudaStream_t st) {
+  double *part = reinterpret_cast<double *>(work);
+  rmse_partial_kernel<<<kRmseBlocks, kRmseThreads, 0, st>>>(nt, u, i, r, X, ldx, T, ldt, f, part);
+  rmse_final_kernel<<<1, 256, 0, st>>>(part, kRmseBlocks, nt, out_dev);
+  return cudaGetLastError();
+}
+
+__global__ void predict_kernel(int64_t nt, const int32_t *u, const int32_t *i, const float *X,
+                               int ldx, const float *T, int ldt, int f, float *out) {
+  const int warps = blockDim.x / 32, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t q = blockIdx.x * (int64_t)warps + w; q < nt; q += (int64_t)gridDim.x * warps) {
+    const float p = dot_warp(X + (int64_t)u[q] * ldx, T + (int64_t)i[q] * ldt, f);
+    if (lane == 0) out[q] = p;
+  }
+}
+
+cudaError_t launch_predict(int64_t nt, const int32_t *u, const int32_t *i, const float *X, int ldx,
+                           const float *T, int ldt, int f, float *out, cudaStream_t st) {
+  if (nt <= 0) return cudaSuccess;
+  predict_kernel<<<kRmseBlocks, kRmseThreads, 0, st>>>(nt, u, i, X, ldx, T, ldt, f, out);
+  return cudaGetLastError();
+}
+
+}  // namespace als

@@ -1,0 +1,176 @@
+/*
+ * als_b200.h -- C ABI of the B200 ALS engine (libGPUALS.so).
+ *
+ * Three layers, all plain C types (no C++ or framework types cross it):
+ *
+ *  1. Drop-in entry points with the exact declarations of the reference
+ *     (IBMSparkGPU/CUDA-MLlib), so an existing caller links unchanged:
+ *       doALSWithCSR   replaces als/src/cuda/als.h:96-103 (body als.cu:1001-1115)
+ *       get_gpu        replaces utilities.h:39 (body utilities.cu:97-136)
+ *       mallocBest     replaces utilities.h:40 (body utilities.cu:73-82)
+ *       freeBest       replaces utilities.h:41 (body utilities.cu:85-95)
+ *     The Spark JNI symbols of als/src/org_apache_spark_ml_recommendation_CuMFJNIInterface.h:31-40
+ *     are exported from the same library (see cumf_jni.h).
+ *
+ *  2. Status-returning engine API on device buffers (new; cuMF has none):
+ *     a resident model with both sides of the rating matrix, the full
+ *     X-then-theta iteration, RMSE and predict.
+ *
+ *  3. als_train: the cuMF-standalone style full-iteration entry on host
+ *     buffers (CSR/CSC arrays, m, n, f, lambda, iterations -> X, theta).
+ *
+ * Conventions: factors are row-major (row u of X is x_u, f floats); CSR row
+ * pointers are int64 in the engine API (int32 in the drop-in one, as in the
+ * reference); column indices int32; ratings float32. Every engine call is
+ * stream-ordered on the stream passed in and does not synchronise unless it
+ * returns a host value. Return codes: ALS_OK or an ALS_ERR_* value;
+ * als_last_error() gives the message of the last failure on this thread.
+ */
+#ifndef ALS_B200_H_
+#define ALS_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- 1. drop-in entry points ---------------- */
+
+/* One ALS half-step, same contract as the reference (als/src/cuda/als.h:98-101):
+ * solves X (m x f, row-major, written to the HOST buffer XTHost) from theta
+ * (n x f, row-major, HOST buffer thetaTHost) and a 0-based CSR of R (m x n)
+ * whose three arrays are DEVICE pointers (or mapped host memory from
+ * mallocBest) that this call FREES, exactly as the reference does
+ * (als.cu:1058, als.cu:1101-1102). lambda is scaled by each row's rating
+ * count (als.cu:905-909). X_BATCH is accepted and ignored: the engine never
+ * materialises the f x f systems in HBM, so it needs no batching.
+ * CUDA failures throw thrust::system_error, as the reference's cudacall does
+ * (als.h:43-53), so the JNI catch block (CuMFJNIInterface.cpp:129-131) still
+ * sees them. Rows without ratings get x_u = 0 (the reference returns NaN). */
+void doALSWithCSR(cudaStream_t cuda_stream, int *csrRowIndex, int *csrColIndex, float *csrVal,
+                  float *thetaTHost, float *XTHost, const int m, const int n, const int f,
+                  const long nnz, const float lambda, const int X_BATCH);
+
+/* Round-robin device choice (utilities.cu:97-136). Unlike the reference it
+ * does not reset every device on first use, which would destroy contexts that
+ * other libraries in the same process hold. Returns -1 without devices. */
+int get_gpu(void);
+/* cudaMalloc, falling back to mapped pinned host memory (utilities.cu:73-82). */
+cudaError_t mallocBest(void **devPtr, size_t size);
+/* Frees either kind of mallocBest allocation (utilities.cu:85-95). */
+cudaError_t freeBest(void *devPtr);
+
+/* ---------------- 2. engine API ---------------- */
+
+enum {
+  ALS_OK = 0,
+  ALS_ERR_INVALID = 1,     /* bad argument                               */
+  ALS_ERR_CUDA = 2,        /* CUDA runtime error (message has details)   */
+  ALS_ERR_UNSUPPORTED = 3, /* e.g. rank outside the kernels' range       */
+  ALS_ERR_NOT_CONVERGED = 4
+};
+
+enum { ALS_PREC_FP32 = 0, ALS_PREC_BF16 = 1, ALS_PREC_FP16 = 2 };
+enum { ALS_SOLVER_CHOLESKY = 0, ALS_SOLVER_CG = 1 };
+enum { ALS_WARM_ZERO = 0, ALS_WARM_PREVIOUS = 1, ALS_WARM_MLP = 2 };
+enum { ALS_SIDE_USERS = 0, ALS_SIDE_ITEMS = 1 };
+
+typedef struct als_options {
+  int32_t precision;    /* ALS_PREC_*: FP32 factors + CUDA-core hermitian, or a
+                           BF16/FP16 factor copy feeding the tensor-core hermitian */
+  int32_t solver;       /* ALS_SOLVER_*                                          */
+  int32_t warm_start;   /* ALS_WARM_* (CG starting point)                        */
+  int32_t cg_max_steps; /* default 16                                            */
+  float cg_tol;         /* CG relative residual target, default 1e-5             */
+  float refine_tol;     /* FP32 relative residual above which an FP64-residual
+                           refinement step runs, default 1e-5                    */
+  int32_t use_graph;    /* capture one iteration as a CUDA graph and replay it  */
+  int32_t reserved[9];
+} als_options;
+
+typedef struct als_stats {
+  uint64_t rows_solved;     /* rows processed since creation / last reset     */
+  uint64_t rows_refined;    /* rows that took the FP64-residual refinement     */
+  uint64_t rows_not_spd;    /* rows whose system had a non-positive pivot      */
+  uint64_t cg_steps;        /* total CG iterations                             */
+  uint64_t cg_fallbacks;    /* CG rows that fell back to Cholesky              */
+  uint64_t reserved[3];
+} als_stats;
+
+void als_default_options(als_options *opt);
+const char *als_last_error(void);
+const char *als_version(void);
+
+typedef struct als_model als_model;
+
+/* Create a resident model. All device arrays are borrowed (the caller keeps
+ * them alive and unchanged for the model's lifetime):
+ *   users side  CSR  (m x n): csr_ptr[m+1], csr_col[nnz], csr_val[nnz]
+ *   items side  CSC  (= CSR of R^T, n x m): csc_ptr[n+1], csc_row[nnz], csc_val[nnz]
+ * The model allocates its factors (X: m x f, theta: n x f, FP32) and scratch. */
+int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t nnz,
+                     const int64_t *csr_ptr, const int32_t *csr_col, const float *csr_val,
+                     const int64_t *csc_ptr, const int32_t *csc_row, const float *csc_val,
+                     const als_options *opt, cudaStream_t stream);
+void als_model_destroy(als_model *model);
+
+/* Copy initial item factors (n x f, row stride ld) from device memory. */
+int als_model_set_theta(als_model *model, const float *d_theta, int32_t ld, cudaStream_t stream);
+/* Copy user factors (m x f) from device memory (warm start for CG). */
+int als_model_set_x(als_model *model, const float *d_x, int32_t ld, cudaStream_t stream);
+
+/* One half-step: ALS_SIDE_USERS solves X from theta, ALS_SIDE_ITEMS solves
+ * theta from X. */
+int als_model_half_step(als_model *model, int32_t side, float lambda, cudaStream_t stream);
+/* `iters` full iterations (users then items). */
+int als_model_iterate(als_model *model, float lambda, int32_t iters, cudaStream_t stream);
+
+/* Borrowed device pointers to the FP32 factors (row stride f). */
+int als_model_factors(als_model *model, float **d_x, float **d_theta);
+/* Per-row status words of the last half-step of each side (see ALS_ROW_*). */
+int als_model_row_flags(als_model *model, int32_t side, const uint32_t **d_flags);
+int als_model_stats(als_model *model, als_stats *out, int32_t reset);
+
+/* Test RMSE over COO triplets (device arrays), FP64 reduction; blocks until
+ * the value is on the host. */
+int als_model_rmse(als_model *model, int64_t nt, const int32_t *d_u, const int32_t *d_i,
+                   const float *d_r, double *rmse_out, cudaStream_t stream);
+
+enum { ALS_ROW_EMPTY = 1, ALS_ROW_NOT_SPD = 2, ALS_ROW_REFINED_F64 = 4, ALS_ROW_CG_FALLBACK = 8 };
+
+/* Stand-alone half-step on caller buffers (no model): src n x f (ld_src),
+ * dst m x f (ld_dst). work must hold als_half_step_work_bytes(m) bytes. */
+size_t als_half_step_work_bytes(int64_t m);
+int als_half_step(int64_t m, int64_t n, int32_t f, const int64_t *d_row_ptr,
+                  const int32_t *d_col, const float *d_val, const float *d_src, int32_t ld_src,
+                  float *d_dst, int32_t ld_dst, float lambda, const als_options *opt,
+                  void *d_work, size_t work_bytes, cudaStream_t stream);
+
+/* RMSE / predict over COO triplets with caller factors. */
+size_t als_rmse_work_bytes(void);
+int als_rmse(int64_t nt, const int32_t *d_u, const int32_t *d_i, const float *d_r,
+             const float *d_x, int32_t ldx, const float *d_theta, int32_t ldt, int32_t f,
+             double *rmse_out, void *d_work, size_t work_bytes, cudaStream_t stream);
+int als_predict(int64_t nt, const int32_t *d_u, const int32_t *d_i, const float *d_x,
+                int32_t ldx, const float *d_theta, int32_t ldt, int32_t f, float *d_out,
+                cudaStream_t stream);
+
+/* ---------------- 3. full training on host buffers ---------------- */
+
+/* cuMF-standalone style entry (not present in the reference; new):
+ * host CSR (m x n) and CSC of the same ratings, initial theta (n x f, row
+ * major, host, overwritten with the result), X_out (m x f, host). Runs
+ * `iterations` full iterations on the current device and stream 0.
+ * stats may be NULL. */
+int als_train(const int64_t *csr_ptr, const int32_t *csr_col, const float *csr_val,
+              const int64_t *csc_ptr, const int32_t *csc_row, const float *csc_val, int64_t m,
+              int64_t n, int32_t f, int64_t nnz, float lambda, int32_t iterations,
+              const als_options *opt, float *X_out, float *theta_inout, als_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALS_B200_H_ */
