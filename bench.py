@@ -272,6 +272,8 @@ def run_engine(args):
         dist.barrier()
     users_ms = np.array([e[0].elapsed_time(e[1]) for e in evs])
     items_ms = np.array([e[1].elapsed_time(e[2]) for e in evs])
+    print("per-step users ms", np.round(users_ms, 2).tolist(), "items ms",
+          np.round(items_ms, 2).tolist(), file=sys.stderr)
     step_ms = users_ms + items_ms
     total_ms = float(step_ms.sum())
     if world > 1:

@@ -61,7 +61,8 @@ class Options(ctypes.Structure):
 
 class Stats(ctypes.Structure):
     _fields_ = [("rows_solved", c_u64), ("rows_refined", c_u64), ("rows_not_spd", c_u64),
-                ("cg_steps", c_u64), ("cg_fallbacks", c_u64), ("reserved", c_u64 * 3)]
+                ("cg_steps", c_u64), ("cg_fallbacks", c_u64), ("kernel_errors", c_u64),
+                ("reserved", c_u64 * 2)]
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
@@ -92,6 +93,8 @@ _sig(lib.als_model_set_theta, c_i32, c_vp, c_vp, c_i32, c_vp)
 _sig(lib.als_model_set_x, c_i32, c_vp, c_vp, c_i32, c_vp)
 _sig(lib.als_model_half_step, c_i32, c_vp, c_i32, c_f32, c_vp)
 _sig(lib.als_model_iterate, c_i32, c_vp, c_f32, c_i32, c_vp)
+_sig(lib.als_model_set_row_range, c_i32, c_vp, c_i32, c_i64, c_i64, c_vp)
+_sig(lib.als_model_sync_lp, c_i32, c_vp, c_i32, c_vp)
 _sig(lib.als_model_factors, c_i32, c_vp, c_vp, c_vp)
 _sig(lib.als_model_row_flags, c_i32, c_vp, c_i32, c_vp)
 _sig(lib.als_model_stats, c_i32, c_vp, c_vp, c_i32)
@@ -337,6 +340,12 @@ class Model:
 
     def half_step(self, side: int, lam: float):
         _check(lib.als_model_half_step(self.handle, side, lam, self.stream))
+
+    def set_row_range(self, side: int, begin: int, end: int):
+        _check(lib.als_model_set_row_range(self.handle, side, begin, end, self.stream))
+
+    def sync_lp(self, side: int):
+        _check(lib.als_model_sync_lp(self.handle, side, self.stream))
 
     def iterate(self, lam: float, iters: int = 1):
         _check(lib.als_model_iterate(self.handle, lam, iters, self.stream))

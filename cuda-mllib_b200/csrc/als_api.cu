@@ -58,6 +58,7 @@ int check_options(const als_options &o, int f) {
 // Scratch for one solve side.
 struct Side {
   int64_t rows = 0, cols = 0;
+  int64_t begin = 0, active = 0;  // rows [begin, begin + active) are solved
   const int64_t *ptr = nullptr;
   const int32_t *idx = nullptr;
   const float *val = nullptr;
@@ -71,7 +72,7 @@ cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, c
                      int ld_src32, const void *src_lp, int ld_lp, float *dst32, void *dst_lp,
                      Counters *ctr, const float *x0, int num_sms, cudaStream_t st) {
   RowsArgs a{};
-  a.m = s.rows;
+  a.m = s.active;
   a.f = f;
   a.lambda = lambda;
   a.row_ptr = s.ptr;
@@ -86,6 +87,7 @@ cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, c
   a.row_flags = s.flags;
   a.counters = ctr;
   a.refine_tol = o.refine_tol;
+  a.error = ctr ? &ctr->error : nullptr;
   cudaError_t e = cudaMemsetAsync(s.queue, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
   const int kind = lp_kind_of(o.precision);
@@ -179,9 +181,9 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
   M->rmse_work = b + oR;
   M->rmse_dev = (double *)(b + oRd);
   Side &U = M->side[ALS_SIDE_USERS], &I = M->side[ALS_SIDE_ITEMS];
-  U.rows = m; U.cols = n; U.ptr = csr_ptr; U.idx = csr_col; U.val = csr_val;
+  U.rows = m; U.cols = n; U.active = m; U.ptr = csr_ptr; U.idx = csr_col; U.val = csr_val;
   U.order = (int32_t *)(b + oOu); U.queue = (unsigned *)(b + oQu); U.flags = (uint32_t *)(b + oFu);
-  I.rows = n; I.cols = m; I.ptr = csc_ptr; I.idx = csc_row; I.val = csc_val;
+  I.rows = n; I.cols = m; I.active = n; I.ptr = csc_ptr; I.idx = csc_row; I.val = csc_val;
   I.order = (int32_t *)(b + oOi); I.queue = (unsigned *)(b + oQi); I.flags = (uint32_t *)(b + oFi);
   e = cudaMemsetAsync(M->block, 0, off, st);
   if (e == cudaSuccess) e = launch_degree_order(U.ptr, m, U.order, U.queue + 1, st);
@@ -234,6 +236,28 @@ static cudaError_t model_half(als_model *M, int side, float lambda, cudaStream_t
   const float *x0 = (M->opt.warm_start == ALS_WARM_PREVIOUS) ? dst32 : nullptr;
   return run_rows(M->side[side], M->f, lambda, M->opt, src32, M->f, src_lp, M->lp_ld, dst32,
                   dst_lp, M->ctr, x0, M->num_sms, st);
+}
+
+int als_model_set_row_range(als_model *M, int32_t side, int64_t begin, int64_t end,
+                            cudaStream_t st) {
+  if (!M || (side != ALS_SIDE_USERS && side != ALS_SIDE_ITEMS)) return fail(ALS_ERR_INVALID, "bad args");
+  Side &S = M->side[side];
+  if (begin < 0 || end < begin || end > S.rows) return fail(ALS_ERR_INVALID, "row range outside the side");
+  if (M->graph) { cudaGraphExecDestroy(M->graph); M->graph = nullptr; }
+  S.begin = begin;
+  S.active = end - begin;
+  ALS_TRY(launch_degree_order(S.ptr, S.active, S.order, S.queue + 1, st, begin), "row range order");
+  return ALS_OK;
+}
+
+int als_model_sync_lp(als_model *M, int32_t side, cudaStream_t st) {
+  if (!M || (side != ALS_SIDE_USERS && side != ALS_SIDE_ITEMS)) return fail(ALS_ERR_INVALID, "bad args");
+  if (!M->X_lp) return ALS_OK;
+  const bool users = side == ALS_SIDE_USERS;
+  ALS_TRY(launch_convert_lp(users ? M->X : M->T, users ? M->m : M->n, M->f, M->f,
+                            users ? M->X_lp : M->T_lp, M->lp_ld, lp_kind_of(M->opt.precision), st),
+          "sync low-precision factors");
+  return ALS_OK;
 }
 
 int als_model_half_step(als_model *M, int32_t side, float lambda, cudaStream_t st) {
@@ -295,6 +319,7 @@ int als_model_stats(als_model *M, als_stats *out, int32_t reset) {
   out->rows_not_spd = c.not_spd;
   out->cg_steps = c.cg_steps;
   out->cg_fallbacks = c.cg_fallback;
+  out->kernel_errors = (uint64_t)(c.error != 0);
   if (reset) ALS_TRY(cudaMemset(M->ctr, 0, sizeof(Counters)), "stats reset");
   return ALS_OK;
 }

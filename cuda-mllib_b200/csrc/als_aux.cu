@@ -20,6 +20,7 @@ __device__ __forceinline__ int degree_bin(int64_t d) {
   return b < kOrderBins ? b : kOrderBins - 1;
 }
 
+// Rows [row_begin, row_begin + m) of the CSR; order[] receives absolute row ids.
 __global__ void order_hist_kernel(const int64_t *row_ptr, int64_t m, unsigned *hist) {
   __shared__ unsigned h[kOrderBins];
   for (int i = threadIdx.x; i < kOrderBins; i += blockDim.x) h[i] = 0;
@@ -44,16 +45,17 @@ __global__ void order_scan_kernel(const unsigned *hist, unsigned *offs) {
 }
 
 __global__ void order_scatter_kernel(const int64_t *row_ptr, int64_t m, unsigned *offs,
-                                     int32_t *order) {
+                                     int32_t *order, int64_t row_begin) {
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < m;
        u += (int64_t)gridDim.x * blockDim.x) {
     const unsigned p = atomicAdd(&offs[degree_bin(row_ptr[u + 1] - row_ptr[u])], 1u);
-    order[p] = (int32_t)u;
+    order[p] = (int32_t)(u + row_begin);
   }
 }
 
 cudaError_t launch_degree_order(const int64_t *row_ptr, int64_t m, int32_t *order,
-                                unsigned *work, cudaStream_t st) {
+                                unsigned *work, cudaStream_t st, int64_t row_begin) {
+  row_ptr += row_begin;
   if (m <= 0) return cudaSuccess;
   cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned) * 2 * kOrderBins, st);
   if (e != cudaSuccess) return e;
@@ -61,7 +63,7 @@ cudaError_t launch_degree_order(const int64_t *row_ptr, int64_t m, int32_t *orde
   const unsigned grid = (unsigned)std::min<int64_t>((m + 255) / 256, (int64_t)sms * 8);
   order_hist_kernel<<<grid, 256, 0, st>>>(row_ptr, m, work);
   order_scan_kernel<<<1, 32, 0, st>>>(work, work + kOrderBins);
-  order_scatter_kernel<<<grid, 256, 0, st>>>(row_ptr, m, work + kOrderBins, order);
+  order_scatter_kernel<<<grid, 256, 0, st>>>(row_ptr, m, work + kOrderBins, order, row_begin);
   return cudaGetLastError();
 }
 

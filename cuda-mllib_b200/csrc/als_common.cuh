@@ -30,6 +30,8 @@ struct Counters {
   unsigned long long not_spd;
   unsigned long long cg_steps;
   unsigned long long cg_fallback;
+  int error;             // sticky kernel error code (1: a bounded wait timed out)
+  int pad;
 };
 
 struct RowsArgs {
@@ -50,6 +52,7 @@ struct RowsArgs {
   uint32_t *row_flags;       // optional per-row status
   Counters *counters;        // optional
   float refine_tol;          // relative residual that triggers FP64 refinement
+  int *error;                // sticky error word (device), may be null
 };
 
 __device__ __forceinline__ float warp_sum(float v) {

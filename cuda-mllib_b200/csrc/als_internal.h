@@ -25,7 +25,7 @@ cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_ma
 // work: 3 * kOrderBins unsigned ints of device scratch.
 constexpr int kOrderBins = 64;
 cudaError_t launch_degree_order(const int64_t *row_ptr, int64_t m, int32_t *order,
-                                unsigned *work, cudaStream_t st);
+                                unsigned *work, cudaStream_t st, int64_t row_begin = 0);
 
 // int32 row pointers (drop-in API) -> int64
 cudaError_t launch_widen_ptr(const int32_t *in, int64_t count, int64_t *out, cudaStream_t st);

@@ -1,11 +1,509 @@
-// Tensor-core (tcgen05) form of the half-step.
+// Tensor-core form of the ALS half-step (sm_100a, tcgen05 + TMEM).
+//
+// Per CSR row u (one CTA per row, persistent over the degree-ordered queue):
+//
+//   gather   the row's item factors (BF16 or FP16 copy, row stride LDP) are
+//            loaded 16 B at a time and stored into a 128B-swizzled MN-major
+//            shared-memory tile: item k is "K row" k, its f factor values run
+//            along M/N. The rating r_uk is patched into element f of the row,
+//            so column f of the product is b_u.
+//   hermitian one elected thread issues tcgen05.mma.kind::f16 with
+//            A = tile^T (M = 128), B = tile (N = NP = roundup16(f+1)), K = 16
+//            per instruction, FP32 accumulation in TMEM:
+//                D[m][n] = sum_k theta_k[m] * [theta_k | r_k][n]
+//            i.e. D[:, :f] = sum theta theta^T and D[:, f] = b_u. Stages of 64
+//            items are double-buffered: tcgen05.commit on a per-buffer mbarrier
+//            releases a buffer once its MMAs completed, while the CTA gathers
+//            the next stage into the other buffer.
+//   solve    D is read back with tcgen05.ld (warp w reads TMEM lanes 32w..),
+//            written to shared memory, and solved by the same register-tile
+//            blocked Cholesky + FP64-residual refinement as the FP32 form.
+//
+// Every mbarrier wait is bounded: on timeout the kernel records an error code
+// and the CTA stops taking rows (no spin is unbounded).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "als_common.cuh"
 #include "als_internal.h"
 
 namespace als {
 
-bool tc_supported(int f) { return false; }
-int tc_padded_ld(int f) { return ((f + 1 + 7) / 8) * 8; }
-cudaError_t launch_rows_tc(const RowsArgs &, int, int, int, float, const float *, int, cudaStream_t) {
+namespace tc {
+
+constexpr int KS = 64;              // items per stage
+constexpr int kStages = 2;
+constexpr unsigned kSpinLimit = 1u << 22;  // try_wait polls (each returns within ~1 us)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Wait until the phase with the given parity has completed. Bounded.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+  const uint32_t a = smem_u32(bar);
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\n"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: 128B swizzle, MN-major canonical layout.
+//   lbo: byte distance between 64-element MN atoms
+//   sbo: byte distance between 8-row K groups
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;  // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulate, A/B 16-bit (fmt 0 = F16,
+// 1 = BF16), both MN-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t make_idesc(int fmt, int n) {
+  return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | (1u << 15) | (1u << 16) |
+         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <typename T>
+__device__ __forceinline__ uint16_t to_bits(float v) {
+  T h = T(v);
+  return *reinterpret_cast<uint16_t *>(&h);
+}
+
+}  // namespace tc
+
+template <int FP>
+struct TcCfg {
+  static constexpr int T8 = FP / 8;
+  static constexpr int NTILES = T8 * (T8 + 1) / 2;
+  static constexpr int NT = ((NTILES + 31) / 32) * 32 < 128 ? 128 : ((NTILES + 31) / 32) * 32;
+  static constexpr int LDS = FP + 1;
+  static constexpr size_t kS = (size_t)FP * LDS * 4;
+};
+
+// Runtime geometry shared by host and device.
+struct TcGeom {
+  int np;        // MMA N
+  int ldp;       // global row stride of the low-precision factors (elements)
+  int chunks;    // 16 B chunks per global row = ldp / 8
+  int atoms;     // MN atoms of 64 elements in the staged tile
+  int stage_bytes;
+  int tmem_cols;
+};
+
+__host__ __device__ inline TcGeom tc_geom(int f) {
+  TcGeom g;
+  g.np = ((f + 1 + 15) / 16) * 16;
+  g.ldp = ((f + 1 + 7) / 8) * 8;
+  g.chunks = g.ldp / 8;
+  const int mn = g.np > 128 ? g.np : 128;
+  g.atoms = (mn + 63) / 64;
+  g.stage_bytes = g.atoms * (tc::KS / 8) * 1024;
+  g.tmem_cols = g.np <= 32 ? 32 : g.np <= 64 ? 64 : g.np <= 128 ? 128 : 256;
+  return g;
+}
+
+// Solver parameters of one launch.
+struct TcSolve {
+  int solver;          // 0: Cholesky, 1: CG with Cholesky fallback
+  int cg_max_steps;
+  float cg_tol2;       // squared relative residual target
+  const float *x0;     // CG starting point (m x ld_x0), or null for zero
+  int ld_x0;
+};
+
+// Sum over the CTA of one value per thread; two slot sets alternate so one
+// barrier per reduction suffices.
+template <int NT>
+__device__ __forceinline__ float cta_sum(float v, float *red, int &slot) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[slot * 8 + (threadIdx.x >> 5)] = v;
+  __syncthreads();
+  float s = 0.f;
+#pragma unroll
+  for (int w = 0; w < NT / 32; ++w) s += red[slot * 8 + w];
+  slot ^= 1;
+  return s;
+}
+
+template <int FP, int NP, typename LP>
+__global__ void __launch_bounds__(TcCfg<FP>::NT)
+rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
+  using C = TcCfg<FP>;
+  constexpr int LDS = C::LDS, NT = C::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // 1024-aligned base for the swizzled stages
+  unsigned char *base = smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023);
+  const size_t stages_bytes = (size_t)tc::kStages * g.stage_bytes;
+  const size_t main_bytes = ((stages_bytes > C::kS ? stages_bytes : C::kS) + 15) / 16 * 16;
+  float *S = reinterpret_cast<float *>(base);   // aliases the stages after the MMAs
+  float *dg = reinterpret_cast<float *>(base + main_bytes);
+  float *bv = dg + FP, *xv = bv + FP, *tmp = xv + FP;
+  float *ps = tmp + FP;                                    // CG direction, NP entries
+  float *red = ps + NP;                                    // 2 x 8 reduction slots
+  double *rd = reinterpret_cast<double *>(red + 16);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(rd + FP);  // [0,1] stages, [2] acc, [3] drain
+  int *misc = reinterpret_cast<int *>(bars + 4);          // slot, bad, tmem base, abort
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int f = a.f;
+  const LP *src = reinterpret_cast<const LP *>(a.src);
+
+  if (tid == 0) {
+    for (int i = 0; i < 4; ++i) tc::mbar_init(&bars[i], 1);
+    misc[3] = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32(&misc[2])),
+                 "r"(g.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  for (int q = tid; q < (int)(stages_bytes / 16); q += NT)
+    reinterpret_cast<uint4 *>(base)[q] = make_uint4(0, 0, 0, 0);
+  for (int q = tid; q < NP; q += NT) ps[q] = 0.f;
+  tc::fence_proxy_async();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = (uint32_t)misc[2];
+
+  int ti = 0, tj = 0;
+  const bool owner = tid < C::NTILES;
+  if (owner) tile_of(tid, ti, tj);
+  unsigned uses0 = 0, uses1 = 0;  // commits issued per stage buffer
+  unsigned acc_phase = 0;
+  int rslot = 0;
+  unsigned long long n_rows = 0, n_ref = 0, n_bad = 0, n_steps = 0, n_fb = 0;
+  const uint32_t lbo = (tc::KS / 8) * 1024, sbo = 1024;
+  const uint32_t stage0 = tc::smem_u32(base);
+  const int rchunk = f >> 3, rpos = f & 7;
+  const int m = tid;                       // this thread's row of A_u (TMEM lane)
+  const bool lane_row = warp < 4;          // warps 0-3 own TMEM lanes 0..127
+  const bool live = lane_row && m < f;
+
+  for (;;) {
+    const int64_t u = next_row(a, &misc[0]);
+    if (u < 0 || misc[3]) break;
+    const int64_t s = a.row_ptr[u], e = a.row_ptr[u + 1];
+    const int64_t d = e - s;
+    ++n_rows;
+    if (d == 0) {
+      for (int i = tid; i < f; i += NT) {
+        a.dst[u * a.ld_dst + i] = 0.f;
+        if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[u * a.ld_dst_lp + i] = LP(0.f);
+      }
+      if (a.row_flags && tid == 0) a.row_flags[u] = kRowEmpty;
+      continue;
+    }
+    // ---------------- gather + MMA over stages ----------------
+    const int nstage = (int)((d + tc::KS - 1) / tc::KS);
+    bool aborted = false;
+    for (int gi = 0; gi < nstage; ++gi) {
+      const int buf = gi & 1;
+      const unsigned used = buf ? uses1 : uses0;
+      // the MMAs of stage gi-2 read this buffer; wait for their commit
+      const bool okw = gi < 2 || tc::mbar_wait(&bars[buf], (used - 1) & 1);
+      const int64_t k0 = s + (int64_t)gi * tc::KS;
+      const int kc = (int)(e - k0 < tc::KS ? e - k0 : tc::KS);
+      const int krows = (kc + 15) & ~15;
+      unsigned char *stg = base + (size_t)buf * g.stage_bytes;
+      if (okw) {
+        for (int q = tid; q < krows * g.chunks; q += NT) {
+          const int k = q / g.chunks, j = q - k * g.chunks;
+          uint4 v = make_uint4(0, 0, 0, 0);
+          if (k < kc) {
+            const int64_t item = a.col[k0 + k];
+            v = __ldg(reinterpret_cast<const uint4 *>(src + item * a.ld_src) + j);
+            if (j == rchunk) reinterpret_cast<uint16_t *>(&v)[rpos] = tc::to_bits<LP>(a.val[k0 + k]);
+          }
+          const int atom = j >> 3, c = j & 7, kg = k >> 3, kr = k & 7;
+          *reinterpret_cast<uint4 *>(stg + atom * lbo + kg * 1024 + kr * 128 + ((c ^ kr) << 4)) = v;
+        }
+      }
+      tc::fence_proxy_async();
+      if (!__syncthreads_and(okw)) { aborted = true; break; }
+      if (tid == 0) {
+        tc::tc_fence_after();
+        const uint32_t sa = stage0 + buf * g.stage_bytes;
+        for (int kk = 0; kk < krows / 16; ++kk) {
+          const uint64_t desc = tc::make_desc(sa + kk * 2 * sbo, lbo, sbo);
+          tc::mma_f16(tmem, desc, desc, idesc, (gi > 0 || kk > 0) ? 1u : 0u);
+        }
+        tc::mma_commit(&bars[buf]);
+        if (gi == nstage - 1) tc::mma_commit(&bars[2]);
+      }
+      if (buf) ++uses1; else ++uses0;
+    }
+    const bool oka = !aborted && tc::mbar_wait(&bars[2], acc_phase);
+    acc_phase ^= 1;
+    if (!__syncthreads_and(oka)) {
+      if (tid == 0) { atomicCAS(a.error, 0, 1); misc[3] = 1; }
+      break;
+    }
+    tc::tc_fence_after();
+    // ---------------- TMEM -> registers: thread m holds row m ----------------
+    float arow[NP];
+#pragma unroll
+    for (int c = 0; c < NP; ++c) arow[c] = 0.f;
+    if (lane_row) {
+#pragma unroll
+      for (int c0 = 0; c0 < NP; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) arow[c0 + q] = v[q];
+      }
+    }
+    tc::tc_fence_before();
+    float bm = 0.f;  // b_u[m] sits in column f
+#pragma unroll
+    for (int c = 0; c < NP; ++c) {
+      if (c == f) bm = arow[c];
+      if (c >= f || !live) arow[c] = 0.f;
+    }
+    if (!live) bm = 0.f;
+    const float reg = a.lambda * (float)d;
+    uint32_t flags = 0;
+    bool solved = false;
+    float xm = 0.f;
+    if (sv.solver == 1) {
+      // ---------------- CG on A_u = arow + reg * I, all in registers ----------------
+      float x = (live && sv.x0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
+      if (!isfinite(x)) x = 0.f;
+      if (live) ps[m] = x;
+      __syncthreads();
+      float q = reg * x;
+#pragma unroll
+      for (int k = 0; k < NP; k += 4) {
+        const float4 p4 = *reinterpret_cast<const float4 *>(ps + k);
+        q = fmaf(arow[k], p4.x, q);
+        q = fmaf(arow[k + 1], p4.y, q);
+        q = fmaf(arow[k + 2], p4.z, q);
+        q = fmaf(arow[k + 3], p4.w, q);
+      }
+      float r = live ? bm - q : 0.f;
+      float p = r;
+      float rr = cta_sum<NT>(r * r, red, rslot);
+      const float bb = cta_sum<NT>(bm * bm, red, rslot);
+      const float target = sv.cg_tol2 * bb;
+      int it = 0;
+      bool conv = rr <= target;
+      while (!conv && it < sv.cg_max_steps) {
+        if (live) ps[m] = p;
+        __syncthreads();
+        float w = reg * p;
+#pragma unroll
+        for (int k = 0; k < NP; k += 4) {
+          const float4 p4 = *reinterpret_cast<const float4 *>(ps + k);
+          w = fmaf(arow[k], p4.x, w);
+          w = fmaf(arow[k + 1], p4.y, w);
+          w = fmaf(arow[k + 2], p4.z, w);
+          w = fmaf(arow[k + 3], p4.w, w);
+        }
+        const float pq = cta_sum<NT>(p * w, red, rslot);
+        if (!(pq > 0.f)) break;  // not positive definite along p: fall back
+        const float alpha = rr / pq;
+        x = fmaf(alpha, p, x);
+        r = fmaf(-alpha, w, r);
+        const float rr2 = cta_sum<NT>(r * r, red, rslot);
+        ++it;
+        conv = rr2 <= target;
+        p = fmaf(rr2 / rr, p, r);
+        rr = rr2;
+      }
+      n_steps += it;
+      if (conv) {
+        solved = true;
+        xm = x;
+      } else {
+        flags |= kRowCgFallback;
+        ++n_fb;
+      }
+      __syncthreads();  // ps reads done before the next row (or S) reuses memory
+    }
+    if (!solved) {
+      // ---------------- register-tile Cholesky + FP64-residual refinement ----------------
+      if (lane_row && m < FP) {
+#pragma unroll
+        for (int c = 0; c < FP; ++c) {
+          const float v = c < NP ? arow[c] : 0.f;
+          S[m * LDS + c] = (m < f && c < f) ? v : (m == c ? 1.f : 0.f);
+        }
+        bv[m] = bm;
+      }
+      __syncthreads();
+      float acc[8][8];
+      if (owner) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const int i = 8 * ti + r, j = 8 * tj + c;
+            float v = S[i * LDS + j];
+            if (i == j && i < f) v += reg;
+            acc[r][c] = v;
+          }
+      }
+      __syncthreads();
+      if (owner && ti == tj) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int i = 8 * ti + r;
+          dg[i] = acc[r][r];
+          xv[i] = bv[i];
+        }
+      }
+      const bool ok = tile_cholesky<FP, LDS, NT>(acc, ti, tj, owner, S, &misc[1]);
+      if (!ok) {
+        for (int i = tid; i < f; i += NT) xv[i] = 0.f;
+        flags |= kRowNotSPD;
+        ++n_bad;
+        __syncthreads();
+      } else {
+        bool refined = false;
+        solve_and_refine<FP, LDS, NT>(S, dg, bv, xv, rd, tmp, f, a.refine_tol, &refined);
+        if (refined) { flags |= kRowRefinedF64; ++n_ref; }
+      }
+      if (live) xm = xv[m];
+    }
+    if (live) {
+      a.dst[u * a.ld_dst + m] = xm;
+      if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[u * a.ld_dst_lp + m] = LP(xm);
+    }
+    if (a.row_flags && tid == 0) a.row_flags[u] = flags;
+    // the next row's gather overwrites S (the stages): make sure all reads are done
+    __syncthreads();
+  }
+  if (a.counters && tid == 0) {
+    atomicAdd(&a.counters->rows, n_rows);
+    if (n_ref) atomicAdd(&a.counters->refined, n_ref);
+    if (n_bad) atomicAdd(&a.counters->not_spd, n_bad);
+    if (n_steps) atomicAdd(&a.counters->cg_steps, n_steps);
+    if (n_fb) atomicAdd(&a.counters->cg_fallback, n_fb);
+  }
+  __syncthreads();
+  if (misc[3]) {  // aborted: drain any MMA still in flight before freeing TMEM
+    if (tid == 0) tc::mma_commit(&bars[3]);
+    tc::mbar_wait(&bars[3], 0);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc::tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(g.tmem_cols));
+  }
+}
+
+bool tc_supported(int f) { return f >= 16 && f <= 128; }
+int tc_padded_ld(int f) { return tc_geom(f).ldp; }
+
+template <int FP, int NP, typename LP>
+static cudaError_t launch_tc_fp(const RowsArgs &a, int lp_kind, const TcSolve &sv, int num_sms,
+                                cudaStream_t st) {
+  using C = TcCfg<FP>;
+  const TcGeom g = tc_geom(a.f);
+  if (g.np != NP) return cudaErrorInvalidValue;
+  const size_t stages = (size_t)tc::kStages * g.stage_bytes;
+  const size_t main_bytes = ((stages > C::kS ? stages : C::kS) + 15) / 16 * 16;
+  const size_t smem = 1024 + main_bytes + 4 * FP * 4 + NP * 4 + 16 * 4 + FP * 8 + 4 * 8 + 64;
+  auto kern = rows_tc_kernel<FP, NP, LP>;
+  cudaError_t err =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, smem);
+  if (err != cudaSuccess) return err;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  per_sm = per_sm < 512 / g.tmem_cols ? per_sm : 512 / g.tmem_cols;  // TMEM columns per SM
+  int64_t grid = (int64_t)num_sms * per_sm;
+  if (grid > a.m) grid = a.m > 0 ? a.m : 1;
+  const uint32_t idesc = tc::make_idesc(lp_kind == kLpBf16 ? 1 : 0, g.np);
+  kern<<<(unsigned)grid, C::NT, smem, st>>>(a, g, idesc, sv);
+  return cudaGetLastError();
+}
+
+template <int FP, int NP>
+static cudaError_t launch_tc_np(const RowsArgs &a, int lp_kind, const TcSolve &sv, int num_sms,
+                                cudaStream_t st) {
+  return lp_kind == kLpBf16 ? launch_tc_fp<FP, NP, __nv_bfloat16>(a, lp_kind, sv, num_sms, st)
+                            : launch_tc_fp<FP, NP, __half>(a, lp_kind, sv, num_sms, st);
+}
+
+cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
+                           float cg_tol, const float *x0, int num_sms, cudaStream_t st) {
+  if (!tc_supported(a.f)) return cudaErrorNotSupported;
+  if (a.ld_src != tc_padded_ld(a.f) || !a.error) return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
+  TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst};
+  const int f = a.f, np = tc_geom(f).np;
+  // (FP, NP): FP >= f is the Cholesky tile extent, NP = roundup16(f + 1) the MMA N
+  if (np == 32) return launch_tc_np<32, 32>(a, lp_kind, sv, num_sms, st);
+  if (np == 48) return launch_tc_np<64, 48>(a, lp_kind, sv, num_sms, st);
+  if (np == 64) return launch_tc_np<64, 64>(a, lp_kind, sv, num_sms, st);
+  if (np == 80) return launch_tc_np<104, 80>(a, lp_kind, sv, num_sms, st);
+  if (np == 96) return launch_tc_np<104, 96>(a, lp_kind, sv, num_sms, st);
+  if (np == 112 && f <= 104) return launch_tc_np<104, 112>(a, lp_kind, sv, num_sms, st);
+  if (np == 112) return launch_tc_np<128, 112>(a, lp_kind, sv, num_sms, st);
+  if (np == 128) return launch_tc_np<128, 128>(a, lp_kind, sv, num_sms, st);
+  if (np == 144) return launch_tc_np<128, 144>(a, lp_kind, sv, num_sms, st);
   return cudaErrorNotSupported;
 }
 

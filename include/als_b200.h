@@ -97,7 +97,9 @@ typedef struct als_stats {
   uint64_t rows_not_spd;    /* rows whose system had a non-positive pivot      */
   uint64_t cg_steps;        /* total CG iterations                             */
   uint64_t cg_fallbacks;    /* CG rows that fell back to Cholesky              */
-  uint64_t reserved[3];
+  uint64_t kernel_errors;   /* 1 if a kernel gave up a bounded wait (results of
+                               that half-step are incomplete)                  */
+  uint64_t reserved[2];
 } als_stats;
 
 void als_default_options(als_options *opt);
@@ -125,6 +127,15 @@ int als_model_set_x(als_model *model, const float *d_x, int32_t ld, cudaStream_t
 /* One half-step: ALS_SIDE_USERS solves X from theta, ALS_SIDE_ITEMS solves
  * theta from X. */
 int als_model_half_step(als_model *model, int32_t side, float lambda, cudaStream_t stream);
+/* Restrict a side's half-steps to rows [begin, end) (default: all rows).
+ * Used to shard rows across GPUs: each rank solves its range, then the ranks
+ * exchange the updated rows (see als_model_sync_lp). */
+int als_model_set_row_range(als_model *model, int32_t side, int64_t begin, int64_t end,
+                            cudaStream_t stream);
+/* Rebuild the BF16/FP16 copy of a side's FP32 factors after they were
+ * changed outside the engine (e.g. rows received from other GPUs). No-op in
+ * the FP32 form. */
+int als_model_sync_lp(als_model *model, int32_t side, cudaStream_t stream);
 /* `iters` full iterations (users then items). */
 int als_model_iterate(als_model *model, float lambda, int32_t iters, cudaStream_t stream);
 

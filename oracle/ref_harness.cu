@@ -11,7 +11,8 @@ extern "C" void doALSWithCSR(cudaStream_t cuda_stream, int *csrRowIndex, int *cs
                              float *csrVal, float *thetaTHost, float *XTHost, const int m,
                              const int n, const int f, const long nnz, const float lambda,
                              const int X_BATCH);
-extern "C" cudaError_t mallocBest(void **devPtr, size_t size);
+// utilities.h gives only get_gpu C linkage; mallocBest keeps C++ linkage.
+cudaError_t mallocBest(void **devPtr, size_t size);
 
 // Returns 0 on success. x_batch must keep batch * f * f below 2^31 (the
 // reference indexes its f x f systems with int).

@@ -160,3 +160,29 @@ def test_lambda_zero_rank_deficient_rows_flagged():
     assert flags[0] & A.ROW_NOT_SPD and np.all(X[0] == 0)
     X_ref, _ = O.half_step(ptr, col, val, th, 0.0)
     assert rel_rows(X[1:], X_ref[1:]).max() < TOL
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP32, A.PREC_BF16])
+def test_row_ranges_compose(ml_small, prec):
+    """Solving a side as two row ranges (what two ranks do) gives the same bits
+    as solving it whole; sync_lp rebuilds the low-precision copy."""
+    r, f = ml_small, 32
+    th0 = A.init_factors(r.n, f, 3)
+    solver = A.SOLVER_CHOLESKY
+    full = A.Model(r, f, A.options(precision=prec, solver=solver), theta0=th0)
+    full.half_step(A.SIDE_USERS, 0.05)
+    X_full = full.factors()[0].clone()
+    part = A.Model(r, f, A.options(precision=prec, solver=solver), theta0=th0)
+    mid = r.m // 3
+    part.set_row_range(A.SIDE_USERS, 0, mid)
+    part.half_step(A.SIDE_USERS, 0.05)
+    part.set_row_range(A.SIDE_USERS, mid, r.m)
+    part.half_step(A.SIDE_USERS, 0.05)
+    part.sync_lp(A.SIDE_USERS)
+    assert torch.equal(part.factors()[0], X_full)
+    full.half_step(A.SIDE_ITEMS, 0.05)
+    part.set_row_range(A.SIDE_ITEMS, 0, r.n)
+    part.half_step(A.SIDE_ITEMS, 0.05)
+    assert torch.equal(part.factors()[1], full.factors()[1])
+    with pytest.raises(A.AlsError):
+        part.set_row_range(A.SIDE_USERS, 5, r.m + 1)
