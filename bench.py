@@ -43,6 +43,9 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0, help="shrink m, n (nnz by scale^2)")
     p.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
     p.add_argument("--solver", default="cholesky", choices=["cholesky", "cg"])
+    p.add_argument("--warm", default="previous", choices=["zero", "previous", "mlp"],
+                   help="CG starting point")
+    p.add_argument("--jacobi", action="store_true", help="diagonal-preconditioned CG")
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -229,7 +232,9 @@ def run_engine(args):
     gen_s = time.perf_counter() - t0
     prec = {"fp32": A.PREC_FP32, "bf16": A.PREC_BF16, "fp16": A.PREC_FP16}[args.precision]
     solver = {"cholesky": A.SOLVER_CHOLESKY, "cg": A.SOLVER_CG}[args.solver]
-    opts = A.options(precision=prec, solver=solver)
+    warm = {"zero": A.WARM_ZERO, "previous": A.WARM_PREVIOUS, "mlp": A.WARM_MLP}[args.warm]
+    opts = A.options(precision=prec, solver=solver, warm_start=warm,
+                     cg_jacobi=1 if args.jacobi else 0)
     stream = torch.cuda.Stream(device=dev)
     th0 = A.init_factors(r.n, f, args.seed + 100)
     with torch.cuda.stream(stream):
@@ -310,7 +315,8 @@ def run_engine(args):
                 "config": {"workload": WORKLOAD if args.scale == 1.0 else f"{args.config} x{args.scale}",
                            "f": f, "lambda": lam, "m": r.m, "n": r.n, "nnz_train": r.nnz,
                            "n_test": int(len(r.test_r)), "precision": args.precision,
-                           "solver": args.solver, "seed": args.seed,
+                           "solver": args.solver, "warm_start": args.warm,
+                           "cg_jacobi": args.jacobi, "seed": args.seed,
                            "l2": "inputs larger than L2 (CSR+CSC %.2f GB per iteration)" % (
                                (r.nnz * 16 + (r.m + r.n) * 8) / 1e9),
                            "parallelism": f"rows sharded x{world}" if world > 1 else "1 GPU",

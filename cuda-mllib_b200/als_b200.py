@@ -56,13 +56,15 @@ c_vp, c_sz = ctypes.c_void_p, ctypes.c_size_t
 class Options(ctypes.Structure):
     _fields_ = [("precision", c_i32), ("solver", c_i32), ("warm_start", c_i32),
                 ("cg_max_steps", c_i32), ("cg_tol", c_f32), ("refine_tol", c_f32),
-                ("use_graph", c_i32), ("reserved", c_i32 * 9)]
+                ("use_graph", c_i32), ("mlp_train_iters", c_i32), ("mlp_steps", c_i32),
+                ("mlp_batch", c_i32), ("mlp_lr", c_f32), ("cg_jacobi", c_i32),
+                ("reserved", c_i32 * 4)]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("rows_solved", c_u64), ("rows_refined", c_u64), ("rows_not_spd", c_u64),
                 ("cg_steps", c_u64), ("cg_fallbacks", c_u64), ("kernel_errors", c_u64),
-                ("reserved", c_u64 * 2)]
+                ("cg_r0_micro", c_u64), ("reserved", c_u64 * 1)]
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
@@ -110,9 +112,22 @@ _sig(lib.als_train, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i
      c_i32, c_vp, c_vp, c_vp, c_vp)
 _sig(lib.doALSWithCSR, None, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int,
      ctypes.c_int, ctypes.c_long, c_f32, ctypes.c_int)
+_sig(lib.als_set_dropin_options, c_i32, c_vp)
+_sig(lib.als_get_dropin_options, c_i32, c_vp)
 _sig(lib.mallocBest, ctypes.c_int, c_vp, c_sz)
 _sig(lib.freeBest, ctypes.c_int, c_vp)
 _sig(lib.get_gpu, ctypes.c_int)
+
+_sig(lib.als_mlp_create, c_i32, c_vp, c_i32, c_i64, c_u64, c_vp)
+_sig(lib.als_mlp_destroy, None, c_vp)
+_sig(lib.als_mlp_feature_stride, c_i32, c_vp)
+_sig(lib.als_mlp_param_count, c_i64, c_i32)
+_sig(lib.als_mlp_get_params, c_i32, c_vp, c_vp, c_vp)
+_sig(lib.als_mlp_set_params, c_i32, c_vp, c_vp, c_vp)
+_sig(lib.als_mlp_gradients, c_i32, c_vp, c_i64, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp)
+_sig(lib.als_mlp_train_step, c_i32, c_vp, c_i64, c_vp, c_vp, c_i32, c_f32, c_vp)
+_sig(lib.als_mlp_forward, c_i32, c_vp, c_i64, c_vp, c_vp, c_i32, c_vp)
+_sig(lib.als_features, c_i32, c_i64, c_i32, c_vp, c_vp, c_vp, c_vp, c_i32, c_i32, c_vp, c_i32, c_vp)
 
 _sig(datalib.als_synth_degrees, c_i32, c_vp, c_vp, c_vp)
 _sig(datalib.als_synth_fill, c_i32, c_vp, c_vp, c_vp, c_vp)
@@ -388,6 +403,75 @@ def _wrap_device(addr: int, shape, dtype):
     return torch.as_tensor(_Iface(), device="cuda")
 
 
+class Mlp:
+    """The learned warm-start network (see als_mlp_* in include/als_b200.h)."""
+
+    def __init__(self, f: int, capacity: int = 8192, seed: int = 1, stream=None):
+        self.f = f
+        self.stream = _stream_handle(stream)
+        h = c_vp()
+        _check(lib.als_mlp_create(ctypes.byref(h), f, capacity, seed, self.stream))
+        self.handle = h
+        self.ldf = int(lib.als_mlp_feature_stride(h))
+        self.nparam = int(lib.als_mlp_param_count(f))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.als_mlp_destroy(self.handle)
+            self.handle = None
+
+    def shapes(self):
+        f, H = self.f, 256
+        return [(H, 2 * f + 1), (H,), (H, H), (H,), (f, H), (f,)]
+
+    def _split(self, flat):
+        out, off = [], 0
+        for sh in self.shapes():
+            k = int(np.prod(sh))
+            out.append(flat[off:off + k].reshape(sh))
+            off += k
+        return out
+
+    def get_params(self):
+        flat = np.empty(self.nparam, np.float32)
+        _check(lib.als_mlp_get_params(self.handle, _ptr(flat), self.stream))
+        return self._split(flat)
+
+    def set_params(self, params):
+        flat = np.concatenate([np.asarray(p, np.float32).ravel() for p in params])
+        _check(lib.als_mlp_set_params(self.handle, _ptr(flat), self.stream))
+
+    def gradients(self, F, T):
+        flat = np.empty(self.nparam, np.float32)
+        loss = c_f64()
+        _check(lib.als_mlp_gradients(self.handle, F.shape[0], _ptr(F), _ptr(T), T.stride(0),
+                                     _ptr(flat), ctypes.byref(loss), self.stream))
+        return self._split(flat), float(loss.value)
+
+    def train_step(self, F, T, lr: float):
+        _check(lib.als_mlp_train_step(self.handle, F.shape[0], _ptr(F), _ptr(T), T.stride(0), lr,
+                                      self.stream))
+
+    def forward(self, F):
+        import torch
+        out = torch.empty((F.shape[0], self.f), dtype=torch.float32, device="cuda")
+        _check(lib.als_mlp_forward(self.handle, F.shape[0], _ptr(F), _ptr(out), self.f,
+                                   self.stream))
+        return out
+
+
+def features(row_ptr, col, val, src, f: int, precision: int, ldf: int, stream=None):
+    """BF16 features [b/n, diag/n, log1p(n)/8] of each CSR row (device tensors);
+    src holds the fixed factors (FP32, BF16 or FP16 per `precision`, row stride
+    src.stride(0) >= f)."""
+    import torch
+    m = row_ptr.shape[0] - 1
+    F = torch.zeros((m, ldf), dtype=torch.bfloat16, device="cuda")
+    _check(lib.als_features(m, f, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(src), src.stride(0),
+                            precision, _ptr(F), ldf, _stream_handle(stream)))
+    return F
+
+
 def half_step(row_ptr, col, val, src, dst, lam: float, opts: Options | None = None, stream=None):
     """Stand-alone FP32 half-step on caller device tensors (no model)."""
     import torch
@@ -450,6 +534,17 @@ def _rt():
             raise ImportError("libcudart.so.12 not found")
         _sig(_cudart.cudaMemcpy, ctypes.c_int, c_vp, c_vp, c_sz, ctypes.c_int)
     return _cudart
+
+
+def set_dropin_options(opts: Options) -> None:
+    """Form used by the drop-in doALSWithCSR (process-wide)."""
+    _check(lib.als_set_dropin_options(ctypes.byref(opts)))
+
+
+def get_dropin_options() -> Options:
+    o = Options()
+    _check(lib.als_get_dropin_options(ctypes.byref(o)))
+    return o
 
 
 def do_als_with_csr(row_ptr32: np.ndarray, col: np.ndarray, val: np.ndarray, theta: np.ndarray,

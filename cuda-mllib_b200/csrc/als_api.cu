@@ -3,6 +3,7 @@
 #include <thrust/system/cuda/error.h>
 #include <thrust/system_error.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -17,6 +18,9 @@ using namespace als;
 namespace {
 
 thread_local std::string g_last_error;
+std::mutex g_dropin_mu;
+als_options g_dropin;       // set on first use from als_default_options
+bool g_dropin_set = false;
 
 int fail(int code, const std::string &msg) {
   g_last_error = msg;
@@ -52,6 +56,13 @@ int check_options(const als_options &o, int f) {
     return fail(ALS_ERR_UNSUPPORTED, "tensor-core form supports rank f in 16..128");
   }
   if (o.cg_max_steps < 0 || o.cg_max_steps > 256) return fail(ALS_ERR_INVALID, "cg_max_steps");
+  if (o.warm_start < ALS_WARM_ZERO || o.warm_start > ALS_WARM_MLP)
+    return fail(ALS_ERR_INVALID, "unknown warm start");
+  if (o.warm_start == ALS_WARM_MLP &&
+      (o.precision == ALS_PREC_FP32 || o.solver != ALS_SOLVER_CG || f > 128))
+    return fail(ALS_ERR_UNSUPPORTED, "the learned warm start needs the tensor-core form with CG");
+  if (o.warm_start == ALS_WARM_MLP && (o.mlp_batch < 64 || o.mlp_steps < 0 || !(o.mlp_lr > 0.f)))
+    return fail(ALS_ERR_INVALID, "bad MLP training options");
   return ALS_OK;
 }
 
@@ -65,12 +76,16 @@ struct Side {
   int32_t *order = nullptr;
   unsigned *queue = nullptr;  // [0]: head, [1..]: order scratch
   uint32_t *flags = nullptr;
+  WsPlan plan;                // work list of the warp-specialised kernel
+  void *plan_mem = nullptr;
+  bool has_plan = false;
 };
 
 // Dispatch one half-step: rows of `s` solved against factor `src`.
 cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, const float *src32,
                      int ld_src32, const void *src_lp, int ld_lp, float *dst32, void *dst_lp,
                      Counters *ctr, const float *x0, int num_sms, cudaStream_t st) {
+  if (s.active <= 0) return cudaSuccess;
   RowsArgs a{};
   a.m = s.active;
   a.f = f;
@@ -98,7 +113,8 @@ cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, c
   }
   a.src = src_lp;
   a.ld_src = ld_lp;
-  return launch_rows_tc(a, kind, o.solver, o.cg_max_steps, o.cg_tol, x0, num_sms, st);
+  return launch_rows_tc(a, kind, o.solver, o.cg_max_steps, o.cg_tol, o.cg_jacobi, x0,
+                        s.has_plan ? &s.plan : nullptr, num_sms, st);
 }
 
 }  // namespace
@@ -118,6 +134,13 @@ struct als_model {
   cudaGraphExec_t graph = nullptr;
   float graph_lambda = 0.f;
   void *block = nullptr;  // single allocation holding everything above
+  // learned warm start: one net per side, features and x0 per side
+  void *net[2] = {nullptr, nullptr};
+  void *feat[2] = {nullptr, nullptr};
+  float *x0[2] = {nullptr, nullptr};
+  int ldf = 0;
+  int halfsteps[2] = {0, 0};
+  void *mlp_block = nullptr;
 };
 
 extern "C" {
@@ -132,9 +155,31 @@ void als_default_options(als_options *o) {
   o->cg_tol = 1e-5f;
   o->refine_tol = 1e-5f;
   o->use_graph = 0;
+  o->mlp_train_iters = 3;
+  o->mlp_steps = 128;
+  o->mlp_batch = 8192;
+  o->mlp_lr = 2e-3f;
+  o->cg_jacobi = 0;
 }
 
 const char *als_last_error(void) { return g_last_error.c_str(); }
+
+int als_get_dropin_options(als_options *o) {
+  if (!o) return fail(ALS_ERR_INVALID, "null options");
+  std::lock_guard<std::mutex> lk(g_dropin_mu);
+  if (!g_dropin_set) { als_default_options(&g_dropin); g_dropin_set = true; }
+  *o = g_dropin;
+  return ALS_OK;
+}
+
+int als_set_dropin_options(const als_options *o) {
+  if (!o) return fail(ALS_ERR_INVALID, "null options");
+  if (o->warm_start == ALS_WARM_MLP) return fail(ALS_ERR_UNSUPPORTED, "no learned warm start in the drop-in call");
+  std::lock_guard<std::mutex> lk(g_dropin_mu);
+  g_dropin = *o;
+  g_dropin_set = true;
+  return ALS_OK;
+}
 const char *als_version(void) { return "als_b200 1.0 (sm_100a)"; }
 
 int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t nnz,
@@ -193,6 +238,40 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
     delete M;
     return cuda_fail(e, "als_model_create");
   }
+  if (kind != kLpNone && tc_ws_supported(f)) {
+    for (int sd = 0; sd < 2 && e == cudaSuccess; ++sd) {
+      Side &S = M->side[sd];
+      e = plan_ws(S.ptr, 0, S.rows, M->num_sms, tc_ws_np(f), (int)S.cols, &S.plan, &S.plan_mem, st);
+      S.has_plan = e == cudaSuccess;
+    }
+    if (e != cudaSuccess) {
+      als_model_destroy(M);
+      return cuda_fail(e, "als_model_create: work plan");
+    }
+  }
+  if (o.warm_start == ALS_WARM_MLP) {
+    const int64_t cap = std::max<int64_t>(o.mlp_batch, 32768);
+    for (int s = 0; s < 2 && e == cudaSuccess; ++s)
+      e = mlp_create(&M->net[s], f, cap, 0x5eedULL + (uint64_t)s, st);
+    if (e == cudaSuccess) {
+      M->ldf = mlp_ldf(M->net[0]);
+      size_t moff = 0;
+      auto mtake = [&](size_t bytes) { size_t p = moff; moff = align_up(moff + bytes, 256); return p; };
+      const size_t oF0 = mtake(2ull * m * M->ldf), oF1 = mtake(2ull * n * M->ldf),
+                   oX0 = mtake(4ull * m * f), oX1 = mtake(4ull * n * f);
+      e = cudaMalloc(&M->mlp_block, moff);
+      if (e == cudaSuccess) {
+        char *mb = (char *)M->mlp_block;
+        M->feat[0] = mb + oF0; M->feat[1] = mb + oF1;
+        M->x0[0] = (float *)(mb + oX0); M->x0[1] = (float *)(mb + oX1);
+        e = cudaMemsetAsync(M->mlp_block, 0, moff, st);
+      }
+    }
+    if (e != cudaSuccess) {
+      als_model_destroy(M);
+      return cuda_fail(e, "als_model_create: learned warm start");
+    }
+  }
   *out = M;
   return ALS_OK;
 }
@@ -200,6 +279,11 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
 void als_model_destroy(als_model *M) {
   if (!M) return;
   if (M->graph) cudaGraphExecDestroy(M->graph);
+  for (int s = 0; s < 2; ++s) {
+    mlp_destroy(M->net[s]);
+    cudaFree(M->side[s].plan_mem);
+  }
+  cudaFree(M->mlp_block);
   cudaFree(M->block);
   delete M;
 }
@@ -233,9 +317,33 @@ static cudaError_t model_half(als_model *M, int side, float lambda, cudaStream_t
   const void *src_lp = users ? M->T_lp : M->X_lp;
   float *dst32 = users ? M->X : M->T;
   void *dst_lp = users ? M->X_lp : M->T_lp;
+  const Side &S = M->side[side];
   const float *x0 = (M->opt.warm_start == ALS_WARM_PREVIOUS) ? dst32 : nullptr;
-  return run_rows(M->side[side], M->f, lambda, M->opt, src32, M->f, src_lp, M->lp_ld, dst32,
-                  dst_lp, M->ctr, x0, M->num_sms, st);
+  bool train = false;
+  if (M->opt.warm_start == ALS_WARM_MLP) {
+    // features of this side's rows against the fixed factor (BF16/FP16 copy)
+    cudaError_t e = mlp_features(S.rows, M->f, S.ptr, S.idx, S.val, src_lp, M->lp_ld,
+                                 lp_kind_of(M->opt.precision), M->feat[side], M->ldf, st);
+    if (e != cudaSuccess) return e;
+    train = M->halfsteps[side] < M->opt.mlp_train_iters;
+    if (train) {
+      x0 = dst32;  // while the net learns, start CG from the previous iterate
+    } else {
+      if ((e = mlp_infer(M->net[side], S.rows, M->feat[side], M->x0[side], M->f, st)) != cudaSuccess)
+        return e;
+      x0 = M->x0[side];
+    }
+  }
+  cudaError_t e = run_rows(S, M->f, lambda, M->opt, src32, M->f, src_lp, M->lp_ld, dst32, dst_lp,
+                           M->ctr, x0, M->num_sms, st);
+  if (e != cudaSuccess) return e;
+  if (M->opt.warm_start == ALS_WARM_MLP) {
+    if (train)
+      e = mlp_train(M->net[side], S.rows, M->opt.mlp_batch, M->opt.mlp_steps, M->feat[side],
+                    dst32, M->f, M->opt.mlp_lr, 77ULL + 1000ULL * M->halfsteps[side] + side, st);
+    ++M->halfsteps[side];
+  }
+  return e;
 }
 
 int als_model_set_row_range(als_model *M, int32_t side, int64_t begin, int64_t end,
@@ -247,6 +355,14 @@ int als_model_set_row_range(als_model *M, int32_t side, int64_t begin, int64_t e
   S.begin = begin;
   S.active = end - begin;
   ALS_TRY(launch_degree_order(S.ptr, S.active, S.order, S.queue + 1, st, begin), "row range order");
+  if (S.has_plan) {
+    cudaFree(S.plan_mem);
+    S.plan_mem = nullptr;
+    cudaError_t e = plan_ws(S.ptr, begin, S.active, M->num_sms, tc_ws_np(M->f), (int)S.cols,
+                            &S.plan, &S.plan_mem, st);
+    S.has_plan = e == cudaSuccess;
+    if (e != cudaSuccess) return cuda_fail(e, "row range plan");
+  }
   return ALS_OK;
 }
 
@@ -271,7 +387,7 @@ int als_model_half_step(als_model *M, int32_t side, float lambda, cudaStream_t s
 int als_model_iterate(als_model *M, float lambda, int32_t iters, cudaStream_t st) {
   if (!M) return fail(ALS_ERR_INVALID, "null model");
   if (iters < 0 || !(lambda >= 0.f)) return fail(ALS_ERR_INVALID, "bad iterations or lambda");
-  if (!M->opt.use_graph || st == 0) {
+  if (!M->opt.use_graph || st == 0 || M->opt.warm_start == ALS_WARM_MLP) {
     for (int it = 0; it < iters; ++it) {
       ALS_TRY(model_half(M, ALS_SIDE_USERS, lambda, st), "iterate (users)");
       ALS_TRY(model_half(M, ALS_SIDE_ITEMS, lambda, st), "iterate (items)");
@@ -320,6 +436,7 @@ int als_model_stats(als_model *M, als_stats *out, int32_t reset) {
   out->cg_steps = c.cg_steps;
   out->cg_fallbacks = c.cg_fallback;
   out->kernel_errors = (uint64_t)(c.error != 0);
+  out->cg_r0_micro = c.r0_micro;
   if (reset) ALS_TRY(cudaMemset(M->ctr, 0, sizeof(Counters)), "stats reset");
   return ALS_OK;
 }
@@ -331,6 +448,65 @@ int als_model_rmse(als_model *M, int64_t nt, const int32_t *u, const int32_t *i,
           "rmse");
   ALS_TRY(cudaMemcpyAsync(out, M->rmse_dev, sizeof(double), cudaMemcpyDeviceToHost, st), "rmse copy");
   ALS_TRY(cudaStreamSynchronize(st), "rmse sync");
+  return ALS_OK;
+}
+
+struct als_mlp {
+  void *net = nullptr;
+  int f = 0;
+};
+
+int als_mlp_create(als_mlp **out, int32_t f, int64_t cap, uint64_t seed, cudaStream_t st) {
+  if (!out || f <= 0 || f > 128 || cap < 64) return fail(ALS_ERR_INVALID, "bad MLP arguments");
+  als_mlp *p = new als_mlp();
+  p->f = f;
+  cudaError_t e = mlp_create(&p->net, f, cap, seed, st);
+  if (e != cudaSuccess) { delete p; return cuda_fail(e, "als_mlp_create"); }
+  *out = p;
+  return ALS_OK;
+}
+void als_mlp_destroy(als_mlp *p) {
+  if (!p) return;
+  mlp_destroy(p->net);
+  delete p;
+}
+int als_mlp_feature_stride(const als_mlp *p) { return p ? mlp_ldf(p->net) : 0; }
+int64_t als_mlp_param_count(int32_t f) { return f > 0 ? mlp_param_count(f) : 0; }
+int als_mlp_get_params(als_mlp *p, float *host, cudaStream_t st) {
+  if (!p || !host) return fail(ALS_ERR_INVALID, "bad args");
+  ALS_TRY(mlp_io(p->net, host, 0, nullptr, st), "als_mlp_get_params");
+  return ALS_OK;
+}
+int als_mlp_set_params(als_mlp *p, const float *host, cudaStream_t st) {
+  if (!p || !host) return fail(ALS_ERR_INVALID, "bad args");
+  ALS_TRY(mlp_io(p->net, const_cast<float *>(host), 2, nullptr, st), "als_mlp_set_params");
+  return ALS_OK;
+}
+int als_mlp_gradients(als_mlp *p, int64_t B, const void *F, const float *T, int32_t ldt,
+                      float *host, double *loss, cudaStream_t st) {
+  if (!p || !F || !T || !host || B < 64 || B % 64 || ldt < p->f) return fail(ALS_ERR_INVALID, "bad args");
+  ALS_TRY(mlp_gradients(p->net, B, F, T, ldt, st), "als_mlp_gradients");
+  ALS_TRY(mlp_io(p->net, host, 1, loss, st), "als_mlp_gradients: copy");
+  return ALS_OK;
+}
+int als_mlp_train_step(als_mlp *p, int64_t B, const void *F, const float *T, int32_t ldt, float lr,
+                       cudaStream_t st) {
+  if (!p || !F || !T || B < 64 || B % 64 || ldt < p->f) return fail(ALS_ERR_INVALID, "bad args");
+  ALS_TRY(mlp_step(p->net, B, F, T, ldt, lr, st), "als_mlp_train_step");
+  return ALS_OK;
+}
+int als_mlp_forward(als_mlp *p, int64_t rows, const void *F, float *out, int32_t ldo,
+                    cudaStream_t st) {
+  if (!p || !F || !out || rows < 0 || ldo < p->f) return fail(ALS_ERR_INVALID, "bad args");
+  ALS_TRY(mlp_infer(p->net, rows, F, out, ldo, st), "als_mlp_forward");
+  return ALS_OK;
+}
+int als_features(int64_t m, int32_t f, const int64_t *ptr, const int32_t *col, const float *val,
+                 const void *src, int32_t ld_src, int32_t prec, void *F, int32_t ldf,
+                 cudaStream_t st) {
+  if (m < 0 || f <= 0 || f > 128 || !ptr || !src || !F || ld_src < f || ldf < 2 * f + 1)
+    return fail(ALS_ERR_INVALID, "bad args");
+  ALS_TRY(mlp_features(m, f, ptr, col, val, src, ld_src, lp_kind_of(prec), F, ldf, st), "als_features");
   return ALS_OK;
 }
 
@@ -490,22 +666,26 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
                              float *thetaTHost, float *XTHost, const int m, const int n,
                              const int f, const long nnz, const float lambda, const int X_BATCH) {
   (void)X_BATCH;
+  als_options o;
+  als_get_dropin_options(&o);
+  if (o.warm_start == ALS_WARM_PREVIOUS) o.warm_start = ALS_WARM_ZERO;  // no previous X here
   if (m < 0 || n <= 0 || f <= 0 || nnz < 0) throw_cuda(cudaErrorInvalidValue, "doALSWithCSR: sizes");
-  if (fp32_padded_rank(f) < 0) throw_cuda(cudaErrorInvalidValue, "doALSWithCSR: rank f must be 1..128");
-  // device buffers: theta, X, widened row pointers, half-step workspace
+  if (check_options(o, f) != ALS_OK) throw_cuda(cudaErrorInvalidValue, als_last_error());
+  const int kind = lp_kind_of(o.precision);
+  const int ldp = kind ? tc_padded_ld(f) : 0;
+  // device buffers: theta (+ low-precision copy), X, widened row pointers, order/queue/counters
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t p = off; off = align_up(off + bytes, 256); return p; };
   const size_t oT = take(sizeof(float) * (size_t)n * f), oX = take(sizeof(float) * (size_t)m * f + 4),
-               oP = take(sizeof(int64_t) * ((size_t)m + 1)), oW = take(als_half_step_work_bytes(m));
+               oP = take(sizeof(int64_t) * ((size_t)m + 1)), oW = take(als_half_step_work_bytes(m)),
+               oL = take(kind ? 2ull * n * ldp : 0);
   char *d = nullptr;
   DROPIN_CALL(cudaMalloc(&d, off), "doALSWithCSR: cudaMalloc");
   DROPIN_CALL(cudaMemcpyAsync(d + oT, thetaTHost, sizeof(float) * (size_t)n * f,
                               cudaMemcpyHostToDevice, st), "doALSWithCSR: theta upload");
   DROPIN_CALL(launch_widen_ptr(csrRowIndex, (int64_t)m + 1, (int64_t *)(d + oP), st),
               "doALSWithCSR: row pointers");
-  als_options o;
-  als_default_options(&o);
-  if (m > 0) {
+  if (m > 0 && kind == kLpNone) {
     int rc = als_half_step(m, n, f, (const int64_t *)(d + oP), csrColIndex, csrVal,
                            (const float *)(d + oT), f, (float *)(d + oX), f, lambda, &o, d + oW,
                            als_half_step_work_bytes(m), st);
@@ -513,9 +693,33 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
       cudaError_t e = cudaGetLastError();
       throw_cuda(e != cudaSuccess ? e : cudaErrorInvalidValue, als_last_error());
     }
+  } else if (m > 0) {
+    // tensor-core form: low-precision copy of theta, a work plan, one launch
+    DROPIN_CALL(launch_convert_lp((const float *)(d + oT), n, f, f, d + oL, ldp, kind, st),
+                "doALSWithCSR: theta copy");
+    Side S;
+    S.rows = m; S.cols = n; S.active = m; S.ptr = (const int64_t *)(d + oP);
+    S.idx = csrColIndex; S.val = csrVal;
+    char *w = d + oW;
+    S.order = (int32_t *)w;
+    S.queue = (unsigned *)(w + align_up(sizeof(int32_t) * m, 256));
+    Counters *ctr = (Counters *)((char *)S.queue + align_up(sizeof(unsigned) * (1 + 3 * kOrderBins), 256));
+    DROPIN_CALL(cudaMemsetAsync(ctr, 0, sizeof(Counters), st), "doALSWithCSR: counters");
+    DROPIN_CALL(launch_degree_order(S.ptr, m, S.order, S.queue + 1, st), "doALSWithCSR: order");
+    if (tc_ws_supported(f)) {
+      DROPIN_CALL(plan_ws(S.ptr, 0, m, device_sm_count(), tc_ws_np(f), n, &S.plan, &S.plan_mem, st),
+                  "doALSWithCSR: plan");
+      S.has_plan = true;
+    }
+    cudaError_t e = run_rows(S, f, lambda, o, (const float *)(d + oT), f, d + oL, ldp,
+                             (float *)(d + oX), nullptr, ctr, nullptr, device_sm_count(), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(S.plan_mem);
+    if (e != cudaSuccess) throw_cuda(e, "doALSWithCSR: tensor-core half-step");
+  }
+  if (m > 0)
     DROPIN_CALL(cudaMemcpyAsync(XTHost, d + oX, sizeof(float) * (size_t)m * f,
                                 cudaMemcpyDeviceToHost, st), "doALSWithCSR: X download");
-  }
   DROPIN_CALL(cudaStreamSynchronize(st), "doALSWithCSR: sync");
   DROPIN_CALL(cudaFree(d), "doALSWithCSR: cudaFree");
   // The callee owns and frees the CSR arrays (reference als.cu:1058, 1101-1102).

@@ -30,6 +30,7 @@ struct Counters {
   unsigned long long not_spd;
   unsigned long long cg_steps;
   unsigned long long cg_fallback;
+  unsigned long long r0_micro;  // sum over CG rows of |b - A x0| / |b| (after scaling), x 1e6
   int error;             // sticky kernel error code (1: a bounded wait timed out)
   int pad;
 };
@@ -54,6 +55,30 @@ struct RowsArgs {
   float refine_tol;          // relative residual that triggers FP64 refinement
   int *error;                // sticky error word (device), may be null
 };
+
+// A group of threads that synchronise together: the whole CTA (id 0) or a
+// warpgroup on its own named barrier. tid is the thread's index in the group.
+struct Bar {
+  int id, n, tid;
+  __device__ __forceinline__ void sync() const {
+    if (id == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+  }
+  // barrier that also returns whether `pred` held on every thread of the group
+  __device__ __forceinline__ bool all(bool pred) const {
+    if (id == 0) return __syncthreads_and(pred);
+    uint32_t r;
+    asm volatile(
+        "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\n"
+        "bar.red.and.pred q, %2, %3, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(n)
+        : "memory");
+    return r != 0;
+  }
+};
+
+__device__ __forceinline__ Bar cta_bar() { return Bar{0, (int)blockDim.x, (int)threadIdx.x}; }
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
@@ -149,10 +174,10 @@ __device__ __forceinline__ void warp_backward(const float *S, float *v, int f) {
 // ---------------------------------------------------------------------------
 template <int FP, int LDS, int NT>
 __device__ bool tile_cholesky(float (&acc)[8][8], int ti, int tj, bool owner, float *S,
-                              int *bad) {
+                              int *bad, const Bar &B) {
   constexpr int T8 = FP / 8;
-  if (threadIdx.x == 0) *bad = 0;
-  __syncthreads();
+  if (B.tid == 0) *bad = 0;
+  B.sync();
   for (int kb = 0; kb < T8; ++kb) {
     // 1. diagonal block
     if (owner && ti == kb && tj == kb) {
@@ -161,9 +186,9 @@ __device__ bool tile_cholesky(float (&acc)[8][8], int ti, int tj, bool owner, fl
 #pragma unroll
         for (int c = 0; c <= r; ++c) S[(8 * kb + r) * LDS + 8 * kb + c] = acc[r][c];
     }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
+    B.sync();
+    if (B.tid < 32) {
+      const int lane = B.tid;
       float *D = S + (8 * kb) * LDS + 8 * kb;
       for (int j = 0; j < 8; ++j) {
         const float d = D[j * LDS + j];
@@ -185,7 +210,7 @@ __device__ bool tile_cholesky(float (&acc)[8][8], int ti, int tj, bool owner, fl
         __syncwarp();
       }
     }
-    __syncthreads();
+    B.sync();
     // 2. panel: L(ti,kb) = tile * D^{-T}
     if (owner && tj == kb && ti > kb) {
       const float *D = S + (8 * kb) * LDS + 8 * kb;
@@ -205,7 +230,7 @@ __device__ bool tile_cholesky(float (&acc)[8][8], int ti, int tj, bool owner, fl
 #pragma unroll
         for (int c = 0; c < 8; ++c) S[(8 * ti + r) * LDS + 8 * kb + c] = acc[r][c];
     }
-    __syncthreads();
+    B.sync();
     // 3. trailing update
     if (owner && tj > kb) {
 #pragma unroll
@@ -222,7 +247,7 @@ __device__ bool tile_cholesky(float (&acc)[8][8], int ti, int tj, bool owner, fl
       }
     }
   }
-  __syncthreads();
+  B.sync();
   return *bad == 0;
 }
 
@@ -237,17 +262,19 @@ __device__ __forceinline__ void tile_of(int t, int &ti, int &tj) {
 // ---------------------------------------------------------------------------
 // Solve with the factor in S, then one FP64-residual refinement step when the
 // FP32 relative residual exceeds tol. Uses the original A_u kept in the strict
-// upper triangle of S plus dg[]. v: on entry b, on exit x. All threads call.
+// upper triangle of S plus dg[]. x: on entry b, on exit the solution. Every
+// thread of the group B calls; red is 64 floats of group-private scratch.
 // ---------------------------------------------------------------------------
 template <int FP, int LDS, int NT>
 __device__ void solve_and_refine(const float *S, const float *dg, const float *b, float *x,
-                                 double *rd, float *tmp, int f, float tol, bool *refined) {
-  const int tid = threadIdx.x;
+                                 double *rd, float *tmp, int f, float tol, bool *refined,
+                                 float *red, const Bar &B) {
+  const int tid = B.tid;
   if (tid < 32) {
     warp_forward<FP, LDS>(S, x, f);
     warp_backward<FP, LDS>(S, x, f);
   }
-  __syncthreads();
+  B.sync();
   // FP32 residual norm vs |b|
   float rr = 0.f, bb = 0.f;
   for (int i = tid; i < f; i += NT) {
@@ -259,17 +286,12 @@ __device__ void solve_and_refine(const float *S, const float *dg, const float *b
   }
   rr = warp_sum(rr);
   bb = warp_sum(bb);
-  __shared__ float red[2][32];
-  if ((tid & 31) == 0) { red[0][tid >> 5] = rr; red[1][tid >> 5] = bb; }
-  __syncthreads();
-  if (tid == 0) {
-    float a = 0.f, c = 0.f;
-    for (int w = 0; w < (NT + 31) / 32; ++w) { a += red[0][w]; c += red[1][w]; }
-    red[0][0] = (a > tol * tol * c) ? 1.f : 0.f;
-  }
-  __syncthreads();
-  const bool need = red[0][0] != 0.f;
-  __syncthreads();
+  if ((tid & 31) == 0) { red[tid >> 5] = rr; red[32 + (tid >> 5)] = bb; }
+  B.sync();
+  float ra = 0.f, rc = 0.f;
+  for (int w = 0; w < (NT + 31) / 32; ++w) { ra += red[w]; rc += red[32 + w]; }
+  const bool need = ra > tol * tol * rc;
+  B.sync();
   *refined = need;
   if (!need) return;
   // FP64 residual r = b - A x, then L L^T d = r in FP32, x += d.
@@ -280,14 +302,14 @@ __device__ void solve_and_refine(const float *S, const float *dg, const float *b
     rd[i] = s;
     tmp[i] = (float)s;
   }
-  __syncthreads();
+  B.sync();
   if (tid < 32) {
     warp_forward<FP, LDS>(S, tmp, f);
     warp_backward<FP, LDS>(S, tmp, f);
   }
-  __syncthreads();
+  B.sync();
   for (int i = tid; i < f; i += NT) x[i] += tmp[i];
-  __syncthreads();
+  B.sync();
 }
 
 }  // namespace als

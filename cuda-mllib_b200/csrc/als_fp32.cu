@@ -53,6 +53,7 @@ rows_fp32_kernel(RowsArgs a, int lp_kind) {
   double *rd = reinterpret_cast<double *>(tmp + FP);
   int *misc = reinterpret_cast<int *>(rd + FP);
 
+  __shared__ float red64[64];
   const int tid = threadIdx.x;
   const int f = a.f;
   int ti = 0, tj = 0;
@@ -155,7 +156,7 @@ rows_fp32_kernel(RowsArgs a, int lp_kind) {
           xv[8 * ti + r] = bvv;
         }
     }
-    const bool ok = tile_cholesky<FP, LDS, NT>(acc, ti, tj, owner, S, &misc[1]);
+    const bool ok = tile_cholesky<FP, LDS, NT>(acc, ti, tj, owner, S, &misc[1], cta_bar());
     uint32_t flags = 0;
     if (!ok) {
       for (int i = tid; i < f; i += NT) xv[i] = 0.f;
@@ -164,7 +165,8 @@ rows_fp32_kernel(RowsArgs a, int lp_kind) {
       __syncthreads();
     } else {
       bool refined = false;
-      solve_and_refine<FP, LDS, NT>(S, dg, bv, xv, rd, tmp, f, a.refine_tol, &refined);
+      solve_and_refine<FP, LDS, NT>(S, dg, bv, xv, rd, tmp, f, a.refine_tol, &refined, red64,
+                                      cta_bar());
       if (refined) { flags |= kRowRefinedF64; ++n_ref; }
     }
     for (int i = tid; i < f; i += NT) {

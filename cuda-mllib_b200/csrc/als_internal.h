@@ -18,8 +18,54 @@ cudaError_t launch_rows_fp32(const RowsArgs &a, int lp_kind, int num_sms, cudaSt
 // outside its range; the caller reports that instead of silently falling back.
 bool tc_supported(int f);
 int tc_padded_ld(int f);  // row stride (elements) of the low-precision factor copy
+struct WsPlan;
 cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
-                           float cg_tol, const float *x0, int num_sms, cudaStream_t st);
+                           float cg_tol, int cg_jacobi, const float *x0, const WsPlan *plan,
+                           int num_sms, cudaStream_t st);
+
+// Solver parameters of one launch.
+struct TcSolve {
+  int solver;          // 0: Cholesky, 1: CG with Cholesky fallback
+  int cg_max_steps;
+  float cg_tol2;       // squared relative residual target
+  const float *x0;     // CG starting point (m x ld_x0), or null for zero
+  int ld_x0;
+  int jacobi;          // 1: diagonal preconditioner
+};
+
+// Work list of the warp-specialised kernel, planned on the host per side:
+// one item per row, or one per chunk of a row split across CTAs.
+struct alignas(16) WorkItem {
+  long long s, e;  // rating range [s, e) of this item
+  int u;           // row
+  int deg;         // the row's total number of ratings (lambda * n_u)
+  int part;        // partial-sum slot of this chunk; -1 when the item is the whole row
+  int heavy;       // index of the split row; -1 otherwise
+};
+
+struct WsPlan {
+  const WorkItem *items = nullptr;
+  int nitems = 0;
+  const int *heavy_nchunks = nullptr;  // per split row: number of chunks
+  const int *heavy_base = nullptr;     // per split row: first partial slot
+  unsigned *heavy_count = nullptr;     // per split row: chunks finished (reset by the last)
+  float *partial = nullptr;            // [slots][128][part_ld]
+  int part_ld = 0;
+  int src_rows = 0;                    // rows of the source factor matrix (TMA bounds)
+};
+
+// Host-side planning of a side's rows [begin, begin + count): items sorted by
+// size, rows above `split` ratings cut into chunks. Device buffers are
+// allocated into `plan` and `mem` (freed with cudaFree(*mem)).
+cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int grid, int np,
+                    int src_rows, WsPlan *plan, void **mem, cudaStream_t st);
+
+// Warp-specialised tensor-core kernel (f in [16, 112]); launch_rows_tc
+// dispatches to it when a plan is given.
+bool tc_ws_supported(int f);
+cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
+                              const WsPlan &plan, int num_sms, cudaStream_t st);
+int tc_ws_np(int f);
 
 // Degree-binned visiting order: rows sorted by descending floor(log2(degree)).
 // work: 3 * kOrderBins unsigned ints of device scratch.
@@ -44,5 +90,24 @@ cudaError_t launch_predict(int64_t nt, const int32_t *u, const int32_t *i, const
                            const float *T, int ldt, int f, float *out, cudaStream_t st);
 
 int device_sm_count();
+
+// Learned CG warm start (als_mlp.cu). The net is opaque to callers.
+cudaError_t mlp_create(void **out, int f, int64_t cap, uint64_t seed, cudaStream_t st);
+void mlp_destroy(void *net);
+int mlp_ldf(const void *net);
+int64_t mlp_nparam(const void *net);
+int *mlp_error(const void *net);
+int64_t mlp_param_count(int f);
+cudaError_t mlp_features(int64_t m, int f, const int64_t *row_ptr, const int32_t *col,
+                         const float *val, const void *src, int ld_src, int lp_kind, void *F,
+                         int ldf, cudaStream_t st);
+cudaError_t mlp_infer(void *net, int64_t m, const void *F, float *X0, int ldx, cudaStream_t st);
+cudaError_t mlp_train(void *net, int64_t m, int64_t batch, int steps, const void *F,
+                      const float *T, int ldt, float lr, uint64_t seed, cudaStream_t st);
+cudaError_t mlp_gradients(void *net, int64_t B, const void *F, const float *T, int ldt,
+                          cudaStream_t st);
+cudaError_t mlp_step(void *net, int64_t B, const void *F, const float *T, int ldt, float lr,
+                     cudaStream_t st);
+cudaError_t mlp_io(void *net, float *host, int what, double *loss, cudaStream_t st);
 
 }  // namespace als

@@ -26,106 +26,11 @@
 
 #include "als_common.cuh"
 #include "als_internal.h"
+#include "als_tcgen05.cuh"
 
 namespace als {
 
-namespace tc {
 
-constexpr int KS = 64;              // items per stage
-constexpr int kStages = 2;
-constexpr unsigned kSpinLimit = 1u << 22;  // try_wait polls (each returns within ~1 us)
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-// Wait until the phase with the given parity has completed. Bounded.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
-  const uint32_t a = smem_u32(bar);
-  for (unsigned it = 0; it < kSpinLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n.reg .pred p;\n"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        "selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-// Shared-memory matrix descriptor: 128B swizzle, MN-major canonical layout.
-//   lbo: byte distance between 64-element MN atoms
-//   sbo: byte distance between 8-row K groups
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version (sm_100)
-  d |= (uint64_t)2 << 61;  // SWIZZLE_128B
-  return d;
-}
-
-// Instruction descriptor, kind::f16: FP32 accumulate, A/B 16-bit (fmt 0 = F16,
-// 1 = BF16), both MN-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t make_idesc(int fmt, int n) {
-  return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | (1u << 15) | (1u << 16) |
-         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                        uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-template <typename T>
-__device__ __forceinline__ uint16_t to_bits(float v) {
-  T h = T(v);
-  return *reinterpret_cast<uint16_t *>(&h);
-}
-
-}  // namespace tc
 
 template <int FP>
 struct TcCfg {
@@ -158,14 +63,7 @@ __host__ __device__ inline TcGeom tc_geom(int f) {
   return g;
 }
 
-// Solver parameters of one launch.
-struct TcSolve {
-  int solver;          // 0: Cholesky, 1: CG with Cholesky fallback
-  int cg_max_steps;
-  float cg_tol2;       // squared relative residual target
-  const float *x0;     // CG starting point (m x ld_x0), or null for zero
-  int ld_x0;
-};
+
 
 // Sum over the CTA of one value per thread; two slot sets alternate so one
 // barrier per reduction suffices.
@@ -200,6 +98,7 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
   uint64_t *bars = reinterpret_cast<uint64_t *>(rd + FP);  // [0,1] stages, [2] acc, [3] drain
   int *misc = reinterpret_cast<int *>(bars + 4);          // slot, bad, tmem base, abort
 
+  __shared__ float red64[64];
   const int tid = threadIdx.x, warp = tid >> 5;
   const int f = a.f;
   const LP *src = reinterpret_cast<const LP *>(a.src);
@@ -410,7 +309,7 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
           xv[i] = bv[i];
         }
       }
-      const bool ok = tile_cholesky<FP, LDS, NT>(acc, ti, tj, owner, S, &misc[1]);
+      const bool ok = tile_cholesky<FP, LDS, NT>(acc, ti, tj, owner, S, &misc[1], cta_bar());
       if (!ok) {
         for (int i = tid; i < f; i += NT) xv[i] = 0.f;
         flags |= kRowNotSPD;
@@ -418,7 +317,8 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
         __syncthreads();
       } else {
         bool refined = false;
-        solve_and_refine<FP, LDS, NT>(S, dg, bv, xv, rd, tmp, f, a.refine_tol, &refined);
+        solve_and_refine<FP, LDS, NT>(S, dg, bv, xv, rd, tmp, f, a.refine_tol, &refined, red64,
+                                      cta_bar());
         if (refined) { flags |= kRowRefinedF64; ++n_ref; }
       }
       if (live) xm = xv[m];
@@ -488,11 +388,13 @@ static cudaError_t launch_tc_np(const RowsArgs &a, int lp_kind, const TcSolve &s
 }
 
 cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
-                           float cg_tol, const float *x0, int num_sms, cudaStream_t st) {
+                           float cg_tol, int cg_jacobi, const float *x0, const WsPlan *plan,
+                           int num_sms, cudaStream_t st) {
   if (!tc_supported(a.f)) return cudaErrorNotSupported;
   if (a.ld_src != tc_padded_ld(a.f) || !a.error) return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
-  TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst};
+  TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst, cg_jacobi};
+  if (plan && tc_ws_supported(a.f)) return launch_rows_tc_ws(a, lp_kind, sv, *plan, num_sms, st);
   const int f = a.f, np = tc_geom(f).np;
   // (FP, NP): FP >= f is the Cholesky tile extent, NP = roundup16(f + 1) the MMA N
   if (np == 32) return launch_tc_np<32, 32>(a, lp_kind, sv, num_sms, st);

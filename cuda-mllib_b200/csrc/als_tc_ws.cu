@@ -1,0 +1,835 @@
+// Warp-specialised tensor-core half-step (sm_100a): gather, hermitian and solve
+// of different rows overlap inside one persistent CTA per SM.
+//
+// Work: a host-planned list of items (rows, or chunks of rows too long for one
+// CTA), largest first, dealt round-robin to the CTAs (LPT balance for
+// power-law degrees). A split row's chunks accumulate partial A_u, b_u into
+// global slots; the chunk that finishes last sums them in chunk order and
+// solves the row.
+//
+//   warp 8      producer: per stage of 64 ratings, lanes 0-15 issue TMA
+//               tile::gather4 loads (4 factor rows x 128 B per instruction,
+//               box one row high, x = 0 and 64) into a 128B-swizzled MN-major
+//               tile (rows beyond the stage read TMA's zero fill); lanes 16-31
+//               write r_uk into the rating atom (column 128). Column indices
+//               and ratings of the next stage are loaded one stage ahead, item
+//               metadata two items ahead, so no dependent load is on the
+//               critical path.
+//   warp 9      MMA issuer (one thread): per stage, tcgen05.mma kind::f16,
+//               A = tile^T (M = 128: atoms 0, 1), B = tile (N = 144: atoms
+//               0, 1 and 16 columns of the rating atom), into one of two TMEM
+//               accumulators (rows alternate); tcgen05.commit frees the stage
+//               and, after the item's last stage, marks the accumulator full.
+//               D[:, :f] = sum theta theta^T, D[:, 128] = b_u; rows and columns
+//               f..127 stay zero.
+//   warps 0-3,  two solver warpgroups, one per accumulator: read D with
+//   4-7         tcgen05.ld (thread m <- TMEM lane m = row m of A_u), release
+//               it, then CG in registers (optionally Jacobi-preconditioned;
+//               Cholesky fallback) or the register-tile Cholesky + FP64-residual
+//               refinement, each on its own named barrier.
+//   warps 10-11 idle (they only join the final barrier).
+//
+// Every mbarrier wait is bounded and gives up when another role aborted; a
+// timeout sets the error word and all roles leave their loops.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "als_common.cuh"
+#include "als_internal.h"
+#include "als_tcgen05.cuh"
+
+namespace als {
+
+namespace ws {
+constexpr int kThreads = 384;
+constexpr int kProdWarp = 8;
+constexpr int kMmaWarp = 9;
+constexpr int NS = 4;                             // shared-memory stages
+constexpr int KS = 64;                            // ratings per stage
+constexpr int kAtom = (KS / 8) * 1024;            // one 64-element MN atom of a stage
+constexpr int kStageBytes = 3 * kAtom;            // theta atoms 0, 1 and the rating atom
+constexpr int kN = 144;                           // MMA N: 128 theta columns + 16 (rating)
+constexpr int kBCol = 128;                        // D[:, 128] = b_u
+constexpr int kBufCols = 256;                     // TMEM columns per accumulator buffer
+constexpr int kTmemCols = 512;                    // two accumulators
+}  // namespace ws
+
+struct WsGeom {
+  int atoms;  // theta atoms loaded per stage: 1 when the factor rows fit 64 columns, else 2
+};
+
+template <int FP, int NP>
+struct WsLayout {
+  static constexpr int LDS = FP + 1;
+  static constexpr size_t kS = (size_t)FP * LDS * 4;
+  static constexpr size_t oDg = kS, oBv = oDg + FP * 4, oXv = oBv + FP * 4, oTmp = oXv + FP * 4;
+  static constexpr size_t oPs = (oTmp + FP * 4 + 15) / 16 * 16;
+  static constexpr int kPs = 128;  // CG broadcast vector: one entry per thread of the warpgroup
+  static_assert(NP <= kPs, "the broadcast vector covers every accumulator column");
+  static constexpr size_t oRed = oPs + kPs * 4;
+  static constexpr size_t oRd = (oRed + 80 * 4 + 7) / 8 * 8;  // 8 CG + 64 refinement + pad
+  static constexpr size_t oMisc = oRd + (size_t)FP * 8;
+  static constexpr size_t kSolver = (oMisc + 16 + 127) / 128 * 128;
+  static constexpr size_t oSolver = (size_t)ws::NS * ws::kStageBytes;
+  static constexpr size_t oCtrl = oSolver + 2 * kSolver;
+  static constexpr size_t kBars = 8 * (2 * ws::NS + 10);  // 16-byte multiple
+  static constexpr size_t kCtrl = kBars + 16 * (ws::NS + 2) + 16;
+  static constexpr size_t kTotal = 1024 + oCtrl + kCtrl;
+};
+
+struct WsCtrl {
+  uint64_t *full, *empty, *acc_full, *acc_empty, *row_full, *row_empty, *drain;
+  int4 *stage_info, *row_info;
+  volatile int *misc;  // [0] TMEM base, [1] abort, [2] producer queue slot
+};
+
+__device__ __forceinline__ void ws_abort(const RowsArgs &a, const WsCtrl &c) {
+  atomicCAS(a.error, 0, 1);
+  c.misc[1] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// producer warp
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void tma_gather4(uint32_t dst, const void *tmap, int x, int y0, int y1,
+                                            int y2, int y3, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3),
+      "r"(tc::smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ WorkItem load_item(const WsPlan &p, long long i) {
+  WorkItem w;
+  if (i < p.nitems) {
+    w = p.items[i];
+  } else {
+    w.s = w.e = 0;
+    w.u = -1;
+    w.deg = w.part = w.heavy = -1;
+  }
+  return w;
+}
+
+// Four column indices (lanes 0-15) or four ratings (lanes 16-31) of stage k0
+// of an item: rating slots 4q..4q+3 with q = lane mod 16. Slots past e give
+// the out-of-range row `oob` (TMA zero fill) / rating 0.
+__device__ __forceinline__ void load_quad(const RowsArgs &a, long long k0, long long e, int lane,
+                                          int oob, int (&cols)[4], float (&vals)[4]) {
+  const int q = lane & 15;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const long long k = k0 + 4 * q + j;
+    const bool in = k < e;
+    if (lane < 16) cols[j] = in ? a.col[k] : oob;
+    else vals[j] = in ? a.val[k] : 0.f;
+  }
+}
+
+template <typename LP>
+__device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &g,
+                           const WsCtrl &c, unsigned char *stages, const void *tmap,
+                           unsigned long long &n_empty_rows) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t st0 = tc::smem_u32(stages);
+  const long long G = gridDim.x;
+  unsigned empty_par = 0, empty_used = 0, row_par = 0, row_used = 0;
+  int slot = 0;
+  long long nrow = 0;
+  long long idx = blockIdx.x;
+  WorkItem cur = load_item(plan, idx), nxt = load_item(plan, idx + G);
+  int cols[4] = {0, 0, 0, 0};
+  float vals[4] = {0.f, 0.f, 0.f, 0.f};
+  if (cur.u >= 0) load_quad(a, cur.s, cur.e, lane, plan.src_rows, cols, vals);
+  while (cur.u >= 0 && !c.misc[1]) {
+    const WorkItem nn = load_item(plan, idx + 2 * G);  // metadata two items ahead
+    if (cur.e == cur.s) {  // a row without ratings: x_u = 0
+      for (int i = lane; i < a.f; i += 32) {
+        a.dst[(long long)cur.u * a.ld_dst + i] = 0.f;
+        if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[(long long)cur.u * a.ld_dst_lp + i] = LP(0.f);
+      }
+      if (lane == 0) {
+        if (a.row_flags) a.row_flags[cur.u] = kRowEmpty;
+        ++n_empty_rows;
+      }
+      if (nxt.u >= 0) load_quad(a, nxt.s, nxt.e, lane, plan.src_rows, cols, vals);
+    } else {
+      const int b = (int)(nrow & 1);
+      ++nrow;
+      if (lane == 0) {
+        bool okr = true;
+        if (row_used & (1u << b)) {
+          okr = tc::mbar_wait_or_abort(&c.row_empty[b], (row_par >> b) & 1, c.misc + 1);
+          row_par ^= 1u << b;
+        }
+        row_used |= 1u << b;
+        if (!okr) c.misc[1] = 1;
+        c.row_info[b] = make_int4(cur.u, cur.deg, cur.part, cur.heavy);
+        tc::mbar_arrive(&c.row_full[b]);
+      }
+      const int nst = (int)((cur.e - cur.s + ws::KS - 1) / ws::KS);
+      for (int gi = 0; gi < nst; ++gi) {
+        const long long k0 = cur.s + (long long)gi * ws::KS;
+        const int kc = (int)(cur.e - k0 < ws::KS ? cur.e - k0 : ws::KS);
+        const int krows = (kc + 15) & ~15;
+        // indices of the next stage (this item's or the next item's first)
+        int ncols[4];
+        float nvals[4];
+        if (gi + 1 < nst) load_quad(a, k0 + ws::KS, cur.e, lane, plan.src_rows, ncols, nvals);
+        else if (nxt.u >= 0) load_quad(a, nxt.s, nxt.e, lane, plan.src_rows, ncols, nvals);
+        bool okw = true;
+        if (empty_used & (1u << slot)) {
+          okw = tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
+          empty_par ^= 1u << slot;
+        }
+        empty_used |= 1u << slot;
+        if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
+        const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
+        if (lane == 0) {
+          c.stage_info[slot] = make_int4(b, krows / 16, gi == 0 ? 1 : 0, gi == nst - 1 ? 1 : 0);
+          mbar_arrive_tx(&c.full[slot], (uint32_t)((krows / 4) * g.atoms * 512));
+        }
+        __syncwarp();
+        const int q = lane & 15;
+        if (lane < 16) {
+          if (4 * q < krows) {
+            const uint32_t dst = sa + (q >> 1) * 1024 + (q & 1) * 512;
+            tma_gather4(dst, tmap, 0, cols[0], cols[1], cols[2], cols[3], &c.full[slot]);
+            if (g.atoms > 1)
+              tma_gather4(dst + ws::kAtom, tmap, 64, cols[0], cols[1], cols[2], cols[3],
+                          &c.full[slot]);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int k = 4 * q + j;
+            if (k < krows) {
+              const uint32_t w0 = k < kc ? (uint32_t)tc::to_bits<LP>(vals[j]) : 0u;
+              const uint32_t dst = sa + 2 * ws::kAtom + (k >> 3) * 1024 + (k & 7) * 128 + ((k & 7) << 4);
+              asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(w0),
+                           "r"(0u), "r"(0u), "r"(0u)
+                           : "memory");
+            }
+          }
+          tc::fence_proxy_async();
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&c.full[slot]);  // releases the rating stores
+        slot = slot + 1 == ws::NS ? 0 : slot + 1;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          cols[j] = ncols[j];
+          vals[j] = nvals[j];
+        }
+      }
+      if (c.misc[1]) break;
+    }
+    idx += G;
+    cur = nxt;
+    nxt = nn;
+  }
+  // end marker for the MMA thread
+  if (empty_used & (1u << slot))
+    tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
+  if (lane == 0) {
+    c.stage_info[slot] = make_int4(-1, 0, 0, 0);
+    mbar_arrive_tx(&c.full[slot], 0);
+    tc::mbar_arrive(&c.full[slot]);
+    // end markers for both solver warpgroups
+    for (int b = 0; b < 2; ++b) {
+      if (row_used & (1u << b))
+        tc::mbar_wait_or_abort(&c.row_empty[b], (row_par >> b) & 1, c.misc + 1);
+      c.row_info[b] = make_int4(-1, 0, 0, 0);
+      tc::mbar_arrive(&c.row_full[b]);
+    }
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// MMA issuer (one thread)
+// ---------------------------------------------------------------------------
+__device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages, uint32_t tmem,
+                       uint32_t idesc) {
+  const uint32_t lbo = (ws::KS / 8) * 1024, sbo = 1024;
+  const uint32_t st0 = tc::smem_u32(stages);
+  unsigned full_par = 0, acc_used = 0, acc_par = 0;
+  int slot = 0;
+  bool ok = true;
+  for (;;) {
+    ok = tc::mbar_wait_or_abort(&c.full[slot], (full_par >> slot) & 1, c.misc + 1);
+    if (!ok) break;
+    full_par ^= 1u << slot;
+    const volatile int *vi = reinterpret_cast<volatile int *>(&c.stage_info[slot]);
+    const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
+    if (info.x < 0) break;
+    const int b = info.x, kmma = info.y, first = info.z, last = info.w;
+    tc::fence_proxy_async();  // the producers' copies become visible to the tensor core
+    if (first) {
+      if (acc_used & (1u << b)) {
+        ok = tc::mbar_wait_or_abort(&c.acc_empty[b], (acc_par >> b) & 1, c.misc + 1);
+        if (!ok) break;
+        acc_par ^= 1u << b;
+      }
+      acc_used |= 1u << b;
+    }
+    tc::tc_fence_after();
+    const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
+    for (int kk = 0; kk < kmma; ++kk) {
+      const uint64_t desc = tc::make_desc(sa + kk * 2 * sbo, lbo, sbo);
+      tc::mma_f16(tmem + (uint32_t)b * ws::kBufCols, desc, desc, idesc,
+                  (first && kk == 0) ? 0u : 1u);
+    }
+    tc::mma_commit(&c.empty[slot]);
+    if (last) tc::mma_commit(&c.acc_full[b]);
+    slot = slot + 1 == ws::NS ? 0 : slot + 1;
+  }
+  if (!ok) ws_abort(a, c);
+  tc::mma_commit(c.drain);  // every MMA issued so far has completed when this fires
+  tc::mbar_wait(c.drain, 0);
+}
+
+// ---------------------------------------------------------------------------
+// solver warpgroup
+// ---------------------------------------------------------------------------
+// Row m of (D + diag I) times the broadcast vector v: four independent FMA
+// chains so the row's dot product is not one 112-long dependency chain.
+template <int NP>
+__device__ __forceinline__ float matvec_row(const float (&arow)[NP], const float *v, float diag,
+                                            float vm) {
+  float q0 = diag * vm, q1 = 0.f, q2 = 0.f, q3 = 0.f;
+#pragma unroll
+  for (int k = 0; k < NP; k += 4) {
+    const float4 p4 = *reinterpret_cast<const float4 *>(v + k);
+    q0 = fmaf(arow[k], p4.x, q0);
+    q1 = fmaf(arow[k + 1], p4.y, q1);
+    q2 = fmaf(arow[k + 2], p4.z, q2);
+    q3 = fmaf(arow[k + 3], p4.w, q3);
+  }
+  return (q0 + q1) + (q2 + q3);
+}
+
+// Sum of two per-thread values over the warpgroup: one barrier.
+__device__ __forceinline__ float2 group_sum2(float a, float b, float *red, int &slot,
+                                             const Bar &B) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  float *r = red + slot * 16;
+  if ((B.tid & 31) == 0) reinterpret_cast<float2 *>(r)[B.tid >> 5] = make_float2(a, b);
+  B.sync();
+  float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const float2 q = reinterpret_cast<const float2 *>(r)[w];
+    t.x += q.x;
+    t.y += q.y;
+  }
+  slot ^= 1;
+  return t;
+}
+
+// Sum of up to four per-thread values over the warpgroup: one barrier.
+__device__ __forceinline__ float4 group_sum4(float4 v, float *red, int &slot, const Bar &B) {
+  v.x = warp_sum(v.x);
+  v.y = warp_sum(v.y);
+  v.z = warp_sum(v.z);
+  v.w = warp_sum(v.w);
+  float *r = red + slot * 16;
+  if ((B.tid & 31) == 0) reinterpret_cast<float4 *>(r)[B.tid >> 5] = v;
+  B.sync();
+  float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const float4 q = reinterpret_cast<const float4 *>(r)[w];
+    t.x += q.x; t.y += q.y; t.z += q.z; t.w += q.w;
+  }
+  slot ^= 1;
+  return t;
+}
+
+// Register-tile Cholesky of the system in S (identity padding beyond f),
+// lambda * n_u added on the diagonal, triangular solves and the FP64-residual
+// refinement; the solution lands in xv. Returns 0, 1 (not SPD: xv = 0) or 2
+// (refined). Kept out of line so the CG loop is register-allocated on its own.
+template <int FP>
+__device__ __noinline__ int ws_cholesky(float *S, float *dg, float *bv, float *xv, float *tmp,
+                                        double *rd, float *red, int *bad, int f, float reg,
+                                        float refine_tol, const Bar &B) {
+  constexpr int LDS = FP + 1, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
+  const int lt = B.tid;
+  int ti = 0, tj = 0;
+  const bool owner = lt < NTILES;
+  if (owner) tile_of(lt, ti, tj);
+  float acc[8][8];
+  if (owner) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) {
+        const int i = 8 * ti + r, j = 8 * tj + cc;
+        float v = S[i * LDS + j];
+        if (i == j && i < f) v += reg;
+        acc[r][cc] = v;
+      }
+  }
+  B.sync();
+  if (owner && ti == tj) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = 8 * ti + r;
+      dg[i] = acc[r][r];
+      xv[i] = bv[i];
+    }
+  }
+  const bool okc = tile_cholesky<FP, LDS, 128>(acc, ti, tj, owner, S, bad, B);
+  if (!okc) {
+    for (int i = lt; i < f; i += 128) xv[i] = 0.f;
+    B.sync();
+    return 1;
+  }
+  bool refined = false;
+  solve_and_refine<FP, LDS, 128>(S, dg, bv, xv, rd, tmp, f, refine_tol, &refined, red, B);
+  return refined ? 2 : 0;
+}
+
+template <int FP, int NP, typename LP>
+__device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &sv,
+                         const WsCtrl &c, unsigned char *mem, uint32_t tmem, int wg) {
+  using L = WsLayout<FP, NP>;
+  constexpr int LDS = L::LDS, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
+  static_assert(NTILES <= 128, "one warpgroup holds at most 128 Cholesky tiles");
+  const int lt = threadIdx.x & 127, wl = (threadIdx.x >> 5) & 3;
+  const Bar B{1 + wg, 128, lt};
+  float *S = reinterpret_cast<float *>(mem);
+  float *dg = reinterpret_cast<float *>(mem + L::oDg), *bv = reinterpret_cast<float *>(mem + L::oBv);
+  float *xv = reinterpret_cast<float *>(mem + L::oXv), *tmp = reinterpret_cast<float *>(mem + L::oTmp);
+  float *ps = reinterpret_cast<float *>(mem + L::oPs), *red = reinterpret_cast<float *>(mem + L::oRed);
+  double *rd = reinterpret_cast<double *>(mem + L::oRd);
+  int *bad = reinterpret_cast<int *>(mem + L::oMisc);
+  const int f = a.f, m = lt;
+  const bool live = m < f;
+  ps[lt] = 0.f;  // L::kPs == 128 entries, one per thread
+  B.sync();
+  unsigned par = 0;
+  int rslot = 0;
+  unsigned long long n_rows = 0, n_ref = 0, n_bad = 0, n_steps = 0, n_fb = 0, n_r0 = 0;
+  const uint32_t tbase = tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)wg * ws::kBufCols;
+  for (;;) {
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[wg], par, c.misc + 1);
+    if (!B.all(ok)) { ws_abort(a, c); break; }
+    const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[wg]);
+    const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
+    B.sync();
+    if (lt == 0) tc::mbar_arrive(&c.row_empty[wg]);
+    if (info.x < 0) break;
+    const int64_t u = info.x;
+    const float reg = a.lambda * (float)info.y;
+    ok = tc::mbar_wait_or_abort(&c.acc_full[wg], par, c.misc + 1);
+    par ^= 1;
+    if (!B.all(ok)) { ws_abort(a, c); break; }
+    tc::tc_fence_after();
+    // Thread m <- row m of D. Columns >= f and rows >= f of D are zero (zero
+    // padding of the gathered factors); column 128 holds b_u.
+    float arow[NP];
+#pragma unroll
+    for (int c0 = 0; c0 < NP; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(tbase + c0, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) arow[c0 + q] = v[q];
+    }
+    float bm;
+    {
+      float v[16];
+      tc::tmem_ld16(tbase + ws::kBCol, v);
+      bm = v[0];
+    }
+    tc::tc_fence_before();
+    tc::mbar_arrive(&c.acc_empty[wg]);  // the accumulator may be overwritten now
+    if (info.z >= 0) {
+      // A chunk of a split row: store the partial sums; the chunk that
+      // finishes last adds all of them, in chunk order, and solves the row.
+      float *P = plan.partial + ((size_t)info.z * 128 + m) * plan.part_ld;
+#pragma unroll
+      for (int cc = 0; cc < NP; cc += 4)
+        __stcg(reinterpret_cast<float4 *>(P + cc),
+               make_float4(arow[cc], arow[cc + 1], arow[cc + 2], arow[cc + 3]));
+      __stcg(P + NP, bm);
+      __threadfence();
+      B.sync();
+      if (lt == 0) {
+        const unsigned done = atomicAdd(&plan.heavy_count[info.w], 1u) + 1;
+        bad[1] = done == (unsigned)plan.heavy_nchunks[info.w] ? 1 : 0;
+      }
+      B.sync();
+      const bool last = bad[1] != 0;
+      B.sync();
+      if (!last) continue;
+      __threadfence();
+      const int base = plan.heavy_base[info.w], nch = plan.heavy_nchunks[info.w];
+#pragma unroll
+      for (int cc = 0; cc < NP; ++cc) arow[cc] = 0.f;
+      bm = 0.f;
+      for (int ch = 0; ch < nch; ++ch) {
+        const float *Q = plan.partial + ((size_t)(base + ch) * 128 + m) * plan.part_ld;
+#pragma unroll
+        for (int cc = 0; cc < NP; cc += 4) {
+          const float4 v = __ldcg(reinterpret_cast<const float4 *>(Q + cc));
+          arow[cc] += v.x;
+          arow[cc + 1] += v.y;
+          arow[cc + 2] += v.z;
+          arow[cc + 3] += v.w;
+        }
+        bm += __ldcg(Q + NP);
+      }
+      if (lt == 0) plan.heavy_count[info.w] = 0;  // ready for the next half-step
+    }
+    ++n_rows;
+    uint32_t flags = 0;
+    bool solved = false;
+    float xm = 0.f;
+    if (sv.solver == 1) {
+      // Conjugate gradients on A_u = D + reg I, preconditioned by diag(A_u)
+      // (Jacobi) unless disabled; three barriers per step.
+      float dinv = live ? 1.f : 0.f;
+      if (sv.jacobi && live) {
+        float dm = 0.f;
+#pragma unroll
+        for (int cc = 0; cc < NP; ++cc)
+          if (cc == m) dm = arow[cc];
+        dinv = 1.f / (dm + reg);
+      }
+      float x = (live && sv.x0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
+      if (!isfinite(x)) x = 0.f;
+      float r = bm;
+      if (sv.x0) {
+        // Scale the warm start optimally along its own direction:
+        // alpha = x0.b / x0.A x0 minimises the A-norm error of alpha * x0, so
+        // the start is never worse than zero in that norm.
+        ps[m] = x;
+        B.sync();
+        const float q0 = live ? matvec_row<NP>(arow, ps, reg, x) : 0.f;
+        const float2 xs = group_sum2(x * bm, x * q0, red, rslot, B);
+        float sc = xs.x / xs.y;
+        if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
+        x *= sc;
+        r = bm - sc * q0;
+      }
+      if (!live) r = 0.f;
+      float z = dinv * r;
+      float p = z;
+      float2 t = group_sum2(r * z, r * r, red, rslot, B);
+      float gamma = t.x;
+      const float bb = group_sum2(bm * bm, 0.f, red, rslot, B).x;
+      const float target = sv.cg_tol2 * bb;
+      if (lt == 0 && bb > 0.f) n_r0 += (unsigned long long)(1e6f * sqrtf(t.y / bb));
+      bool conv = t.y <= target;
+      int it = 0;
+      while (!conv && it < sv.cg_max_steps) {
+        ps[m] = p;
+        B.sync();
+        const float w = matvec_row<NP>(arow, ps, reg, p);
+        const float pq = group_sum2(p * w, 0.f, red, rslot, B).x;
+        if (!(pq > 0.f)) break;  // not positive definite along p: fall back
+        const float alpha = gamma / pq;
+        x = fmaf(alpha, p, x);
+        r = fmaf(-alpha, w, r);
+        z = dinv * r;
+        t = group_sum2(r * z, r * r, red, rslot, B);
+        ++it;
+        conv = t.y <= target;
+        p = fmaf(t.x / gamma, p, z);
+        gamma = t.x;
+      }
+      if (lt == 0) n_steps += it;
+      if (conv) {
+        solved = true;
+        xm = x;
+      } else {
+        flags |= kRowCgFallback;
+        if (lt == 0) ++n_fb;
+      }
+      B.sync();
+    }
+    if (!solved) {
+      if (m < FP) {
+#pragma unroll
+        for (int cc = 0; cc < FP; ++cc) {
+          const float v = cc < NP ? arow[cc] : 0.f;
+          S[m * LDS + cc] = (m < f && cc < f) ? v : (m == cc ? 1.f : 0.f);
+        }
+        bv[m] = bm;
+      }
+      B.sync();
+      const int res = ws_cholesky<FP>(S, dg, bv, xv, tmp, rd, red + 8, bad, f, reg, a.refine_tol, B);
+      if (res == 1) {
+        flags |= kRowNotSPD;
+        if (lt == 0) ++n_bad;
+      } else if (res == 2) {
+        flags |= kRowRefinedF64;
+        if (lt == 0) ++n_ref;
+      }
+      if (live) xm = xv[m];
+      B.sync();
+    }
+    if (live) {
+      a.dst[u * a.ld_dst + m] = xm;
+      if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[u * a.ld_dst_lp + m] = LP(xm);
+    }
+    if (a.row_flags && lt == 0) a.row_flags[u] = flags;
+  }
+  if (a.counters && lt == 0) {
+    atomicAdd(&a.counters->rows, n_rows);
+    if (n_ref) atomicAdd(&a.counters->refined, n_ref);
+    if (n_bad) atomicAdd(&a.counters->not_spd, n_bad);
+    if (n_steps) atomicAdd(&a.counters->cg_steps, n_steps);
+    if (n_fb) atomicAdd(&a.counters->cg_fallback, n_fb);
+    if (n_r0) atomicAdd(&a.counters->r0_micro, n_r0);
+  }
+}
+
+template <int FP, int NP, typename LP>
+__global__ void __launch_bounds__(ws::kThreads, 1)
+rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan,
+                  const __grid_constant__ CUtensorMap tmap) {
+  using L = WsLayout<FP, NP>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char *base = smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023);
+  unsigned char *ctrl = base + L::oCtrl;
+  WsCtrl c;
+  c.full = reinterpret_cast<uint64_t *>(ctrl);
+  c.empty = c.full + ws::NS;
+  c.acc_full = c.empty + ws::NS;
+  c.acc_empty = c.acc_full + 2;
+  c.row_full = c.acc_empty + 2;
+  c.row_empty = c.row_full + 2;
+  c.drain = c.row_empty + 2;
+  c.stage_info = reinterpret_cast<int4 *>(ctrl + L::kBars);
+  c.row_info = c.stage_info + ws::NS;
+  c.misc = reinterpret_cast<volatile int *>(c.row_info + 2);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  if (tid == 0) {
+    for (int i = 0; i < ws::NS; ++i) {
+      tc::mbar_init(&c.full[i], 2);  // expect-tx arrive + the arrive releasing the rating stores
+      tc::mbar_init(&c.empty[i], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&c.acc_full[b], 1);
+      tc::mbar_init(&c.acc_empty[b], 128);
+      tc::mbar_init(&c.row_full[b], 1);
+      tc::mbar_init(&c.row_empty[b], 1);
+    }
+    tc::mbar_init(c.drain, 1);
+    c.misc[1] = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == ws::kMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32((const void *)&c.misc[0])),
+                 "r"(ws::kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  for (int q = tid; q < ws::NS * ws::kStageBytes / 16; q += ws::kThreads)
+    reinterpret_cast<uint4 *>(base)[q] = make_uint4(0, 0, 0, 0);
+  tc::fence_proxy_async();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = (uint32_t)c.misc[0];
+  unsigned long long n_empty = 0;
+
+  if (warp == ws::kMmaWarp) {
+    if ((tid & 31) == 0) ws_mma(a, c, base, tmem, idesc);
+    __syncwarp();
+  } else if (warp == ws::kProdWarp) {
+    ws_produce<LP>(a, plan, g, c, base, &tmap, n_empty);
+    if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
+  } else if (warp < 8) {
+    ws_solve<FP, NP, LP>(a, plan, sv, c, base + L::oSolver + (size_t)(warp >> 2) * L::kSolver,
+                         tmem, warp >> 2);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == ws::kMmaWarp) {
+    tc::tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(ws::kTmemCols));
+  }
+}
+
+bool tc_ws_supported(int f) { return f >= 16 && f <= 112; }
+int tc_ws_np(int f) { return ((f + 15) / 16) * 16; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static cudaError_t encode_rows_map(CUtensorMap *map, const void *src, int rows, int ldp,
+                                   int lp_kind) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return cudaErrorNotSupported;
+    fn = (EncodeTiledFn)p;
+  }
+  // rows x ldp elements (16-bit), row stride 2*ldp bytes; box 64 x 1 (gather4 loads 4 rows)
+  const cuuint64_t dims[2] = {(cuuint64_t)ldp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ldp * 2};
+  const cuuint32_t box[2] = {64, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, lp_kind == kLpBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                        2, const_cast<void *>(src), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int FP, int NP, typename LP>
+static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
+                             const WsPlan &plan, int num_sms, cudaStream_t st) {
+  using L = WsLayout<FP, NP>;
+  WsGeom g;
+  g.atoms = a.ld_src <= 64 ? 1 : 2;
+  if (a.ld_src % 8 != 0 || a.ld_src > 128 || NP < a.f || FP < a.f || plan.part_ld < NP + 1)
+    return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
+  CUtensorMap map;
+  cudaError_t err = encode_rows_map(&map, a.src, plan.src_rows, a.ld_src, lp_kind);
+  if (err != cudaSuccess) return err;
+  auto kern = rows_tc_ws_kernel<FP, NP, LP>;
+  err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kTotal);
+  if (err != cudaSuccess) return err;
+  int64_t grid = num_sms;
+  if (grid > plan.nitems) grid = plan.nitems > 0 ? plan.nitems : 1;
+  const uint32_t idesc = tc::make_idesc(lp_kind == kLpBf16 ? 1 : 0, ws::kN);
+  kern<<<(unsigned)grid, ws::kThreads, L::kTotal, st>>>(a, idesc, sv, g, plan, map);
+  return cudaGetLastError();
+}
+
+template <int FP, int NP>
+static cudaError_t launch_ws_np(const RowsArgs &a, int lp_kind, const TcSolve &sv,
+                                const WsPlan &plan, int num_sms, cudaStream_t st) {
+  return lp_kind == kLpBf16 ? launch_ws<FP, NP, __nv_bfloat16>(a, lp_kind, sv, plan, num_sms, st)
+                            : launch_ws<FP, NP, __half>(a, lp_kind, sv, plan, num_sms, st);
+}
+
+// f in [16, 112]: NP = roundup16(f) accumulator columns are read back per row,
+// FP >= f is the Cholesky tile extent.
+cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
+                              const WsPlan &plan, int num_sms, cudaStream_t st) {
+  const int f = a.f;
+  if (!tc_ws_supported(f)) return cudaErrorNotSupported;
+  if (plan.nitems <= 0) return cudaSuccess;
+  switch (tc_ws_np(f)) {
+    case 16: return launch_ws_np<32, 16>(a, lp_kind, sv, plan, num_sms, st);
+    case 32: return launch_ws_np<32, 32>(a, lp_kind, sv, plan, num_sms, st);
+    case 48: return launch_ws_np<64, 48>(a, lp_kind, sv, plan, num_sms, st);
+    case 64: return launch_ws_np<64, 64>(a, lp_kind, sv, plan, num_sms, st);
+    case 80: return launch_ws_np<104, 80>(a, lp_kind, sv, plan, num_sms, st);
+    case 96: return launch_ws_np<104, 96>(a, lp_kind, sv, plan, num_sms, st);
+    case 112: return f <= 104 ? launch_ws_np<104, 112>(a, lp_kind, sv, plan, num_sms, st)
+                              : launch_ws_np<112, 112>(a, lp_kind, sv, plan, num_sms, st);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host planning of the work list
+// ---------------------------------------------------------------------------
+cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int grid, int np,
+                    int src_rows, WsPlan *plan, void **mem, cudaStream_t st) {
+  *mem = nullptr;
+  *plan = WsPlan();
+  plan->src_rows = src_rows;
+  plan->part_ld = np + 4;
+  if (count <= 0) return cudaSuccess;
+  std::vector<int64_t> ptr((size_t)count + 1);
+  cudaError_t e = cudaMemcpyAsync(ptr.data(), d_row_ptr + begin, sizeof(int64_t) * (count + 1),
+                                  cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  const int64_t nnz = ptr[(size_t)count] - ptr[0];
+  // rows longer than a quarter of a CTA's fair share are split
+  const int64_t split = std::max<int64_t>(8192, (nnz + 4LL * grid - 1) / (4LL * grid));
+  std::vector<WorkItem> items;
+  items.reserve((size_t)count + 64);
+  std::vector<int> hn, hb;
+  int slots = 0;
+  for (int64_t r = 0; r < count; ++r) {
+    const int64_t s = ptr[(size_t)r], e2 = ptr[(size_t)r + 1], d = e2 - s;
+    const int u = (int)(begin + r);
+    if (d > split) {
+      const int nch = (int)((d + split - 1) / split);
+      const int h = (int)hn.size();
+      hn.push_back(nch);
+      hb.push_back(slots);
+      for (int ch = 0; ch < nch; ++ch) {
+        WorkItem w;
+        w.s = s + ch * split;
+        w.e = std::min<int64_t>(e2, s + (ch + 1) * split);
+        w.u = u;
+        w.deg = (int)d;
+        w.part = slots + ch;
+        w.heavy = h;
+        items.push_back(w);
+      }
+      slots += nch;
+    } else {
+      WorkItem w;
+      w.s = s;
+      w.e = e2;
+      w.u = u;
+      w.deg = (int)d;
+      w.part = -1;
+      w.heavy = -1;
+      items.push_back(w);
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const WorkItem &x, const WorkItem &y) {
+    return x.e - x.s > y.e - y.s;
+  });
+  const size_t nh = hn.size();
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t oI = 0, oN = al(sizeof(WorkItem) * items.size()), oB = oN + al(4 * (nh + 1)),
+               oC = oB + al(4 * (nh + 1)), oP = oC + al(4 * (nh + 1)),
+               total = oP + al(sizeof(float) * (size_t)slots * 128 * plan->part_ld + 16);
+  char *d = nullptr;
+  if ((e = cudaMalloc(&d, total)) != cudaSuccess) return e;
+  e = cudaMemcpyAsync(d + oI, items.data(), sizeof(WorkItem) * items.size(),
+                      cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && nh)
+    e = cudaMemcpyAsync(d + oN, hn.data(), 4 * nh, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && nh)
+    e = cudaMemcpyAsync(d + oB, hb.data(), 4 * nh, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d + oC, 0, 4 * (nh + 1), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors go out of scope
+  if (e != cudaSuccess) { cudaFree(d); return e; }
+  plan->items = (const WorkItem *)(d + oI);
+  plan->nitems = (int)items.size();
+  plan->heavy_nchunks = (const int *)(d + oN);
+  plan->heavy_base = (const int *)(d + oB);
+  plan->heavy_count = (unsigned *)(d + oC);
+  plan->partial = (float *)(d + oP);
+  *mem = d;
+  return cudaSuccess;
+}
+
+}  // namespace als

@@ -88,7 +88,14 @@ typedef struct als_options {
   float refine_tol;     /* FP32 relative residual above which an FP64-residual
                            refinement step runs, default 1e-5                    */
   int32_t use_graph;    /* capture one iteration as a CUDA graph and replay it  */
-  int32_t reserved[9];
+  /* learned warm start (ALS_WARM_MLP, tensor-core form with CG) */
+  int32_t mlp_train_iters; /* iterations whose solves train the MLP (default 3)   */
+  int32_t mlp_steps;       /* Adam steps per half-step while training (default 128) */
+  int32_t mlp_batch;       /* rows per Adam step (default 8192)                   */
+  float mlp_lr;            /* Adam learning rate (default 2e-3)                   */
+  int32_t cg_jacobi;       /* 1: diagonal (Jacobi) preconditioner for CG (default 0:
+                              it slowed convergence on the benchmark matrices) */
+  int32_t reserved[4];
 } als_options;
 
 typedef struct als_stats {
@@ -99,10 +106,19 @@ typedef struct als_stats {
   uint64_t cg_fallbacks;    /* CG rows that fell back to Cholesky              */
   uint64_t kernel_errors;   /* 1 if a kernel gave up a bounded wait (results of
                                that half-step are incomplete)                  */
-  uint64_t reserved[2];
+  uint64_t cg_r0_micro;     /* sum over CG rows of the starting relative residual
+                               |b - A x0| / |b| (x0 after optimal scaling), x 1e6:
+                               a measure of the warm start's quality          */
+  uint64_t reserved[1];
 } als_stats;
 
 void als_default_options(als_options *opt);
+/* Options the drop-in doALSWithCSR uses (process-wide; default: the FP32
+ * form with Cholesky, which meets the reference's 1e-3 parity). A Spark
+ * deployment can select the tensor-core form (BF16/FP16 + CG) here without
+ * changing the call. No counterpart in the reference. */
+int als_set_dropin_options(const als_options *opt);
+int als_get_dropin_options(als_options *opt);
 const char *als_last_error(void);
 const char *als_version(void);
 
@@ -168,6 +184,35 @@ int als_rmse(int64_t nt, const int32_t *d_u, const int32_t *d_i, const float *d_
 int als_predict(int64_t nt, const int32_t *d_u, const int32_t *d_i, const float *d_x,
                 int32_t ldx, const float *d_theta, int32_t ldt, int32_t f, float *d_out,
                 cudaStream_t stream);
+
+/* Learned warm start: the MLP that maps a row's features
+ * [b_u / n_u, diag(A_u) / n_u, log1p(n_u) / 8] (2f+1 values, BF16, row stride
+ * als_mlp_feature_stride) to x0 (f floats). Layers 2f+1 -> 256 -> 256 -> f with
+ * GELU, BF16 weights and activations, FP32 accumulation; tensor-core kernels
+ * for forward, backward and Adam. No counterpart in the reference. */
+typedef struct als_mlp als_mlp;
+int als_mlp_create(als_mlp **out, int32_t f, int64_t batch_capacity, uint64_t seed,
+                   cudaStream_t stream);
+void als_mlp_destroy(als_mlp *mlp);
+int als_mlp_feature_stride(const als_mlp *mlp);
+int64_t als_mlp_param_count(int32_t f);
+/* host <-> parameters, unpadded, in the order W1 [256 x (2f+1)], b1 [256],
+ * W2 [256 x 256], b2 [256], W3 [f x 256], b3 [f] (W[out][in]) */
+int als_mlp_get_params(als_mlp *mlp, float *host, cudaStream_t stream);
+int als_mlp_set_params(als_mlp *mlp, const float *host, cudaStream_t stream);
+/* loss = mean_b |y_b - t_b|^2 / f and its gradients (same layout as the
+ * parameters) for `batch` rows, without updating; batch a multiple of 64 */
+int als_mlp_gradients(als_mlp *mlp, int64_t batch, const void *d_features, const float *d_targets,
+                      int32_t ldt, float *host_grads, double *loss, cudaStream_t stream);
+int als_mlp_train_step(als_mlp *mlp, int64_t batch, const void *d_features,
+                       const float *d_targets, int32_t ldt, float lr, cudaStream_t stream);
+int als_mlp_forward(als_mlp *mlp, int64_t rows, const void *d_features, float *d_out, int32_t ldo,
+                    cudaStream_t stream);
+/* features of rows [0, m) of a CSR against source factors d_src (kind:
+ * ALS_PREC_FP32 / BF16 / FP16, row stride ld_src) into d_features (BF16). */
+int als_features(int64_t m, int32_t f, const int64_t *d_row_ptr, const int32_t *d_col,
+                 const float *d_val, const void *d_src, int32_t ld_src, int32_t src_precision,
+                 void *d_features, int32_t ldf, cudaStream_t stream);
 
 /* ---------------- 3. full training on host buffers ---------------- */
 
