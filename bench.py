@@ -41,8 +41,8 @@ def parse():
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--config", default="netflix")
     p.add_argument("--scale", type=float, default=1.0, help="shrink m, n (nnz by scale^2)")
-    p.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
-    p.add_argument("--solver", default="cholesky", choices=["cholesky", "cg"])
+    p.add_argument("--precision", default="bf16", choices=["fp32", "bf16", "fp16"])
+    p.add_argument("--solver", default="cg", choices=["cholesky", "cg"])
     p.add_argument("--warm", default="previous", choices=["zero", "previous", "mlp"],
                    help="CG starting point")
     p.add_argument("--jacobi", action="store_true", help="diagonal-preconditioned CG")
@@ -291,6 +291,12 @@ def run_engine(args):
     rmse = model.rmse()
     flop_iter = A.flop_per_iteration(r, f)
     gflops = flop_iter * args.steps / (total_ms / 1e3) / 1e9
+    # launches of this library's kernels per timed iteration: one rows kernel per
+    # half-step; with the learned warm start also the features pass and the
+    # three MLP GEMMs per inference chunk of 32,768 rows
+    launches_per_step = 2
+    if args.warm == "mlp":
+        launches_per_step += 2 + 3 * (-(-r.m // 32768) + -(-r.n // 32768))
 
     # roofline of the dominant kernel: the fused rows kernel, one launch per half-step
     hbm, tf_burst, tf_sust, src = peaks()
@@ -322,10 +328,16 @@ def run_engine(args):
                            "parallelism": f"rows sharded x{world}" if world > 1 else "1 GPU",
                            "generation_s": round(gen_s, 2)},
                 "rmse": round(rmse, 6), "roofline": roof,
-                "gpu_launches": 2 * args.steps, "clocks": ck_sum, "solver_stats": stats}
+                "gpu_launches": launches_per_step * args.steps, "clocks": ck_sum,
+                "solver_stats": stats,
+                "cg_steps_per_row": round(stats["cg_steps"] / max(1, stats["rows_solved"]), 3)}
 
-    # e2e through the drop-in entry point with host buffers (rank 0, 1 GPU path)
+    # e2e through the drop-in entry point with host buffers (rank 0, 1 GPU path),
+    # in the same precision and solver (the drop-in call has no previous X: CG
+    # starts from zero there)
     if rank == 0 and not args.no_e2e:
+        A.set_dropin_options(A.options(precision=prec, solver=solver, warm_start=A.WARM_ZERO,
+                                       cg_jacobi=1 if args.jacobi else 0))
         X = model.factors()[0].cpu().numpy()
         T = model.factors()[1].cpu().numpy()
         ptr32 = r.csr_ptr.astype(np.int32)
@@ -348,7 +360,7 @@ def run_engine(args):
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "sec_per_iter": round(e2e_s, 4),
                        "path": "doALSWithCSR x2 (users, items): CSR upload to mallocBest memory, "
-                               "theta upload, X download; wall clock, FP32 form"}
+                               "theta upload, X download; wall clock; same form (CG from zero)"}
         line["gpu_launches"] += 0
 
     if rank == 0 and not args.no_cpu_baseline:

@@ -186,3 +186,24 @@ def test_row_ranges_compose(ml_small, prec):
     assert torch.equal(part.factors()[1], full.factors()[1])
     with pytest.raises(A.AlsError):
         part.set_row_range(A.SIDE_USERS, 5, r.m + 1)
+
+
+def test_dropin_tensor_core_form(ml_small):
+    """doALSWithCSR switched to the tensor-core form (BF16 copy of theta, CG
+    from zero) through the process-wide drop-in options; the FP32 default is
+    restored afterwards."""
+    import torch
+    r, f = ml_small, 32
+    th = A.init_factors(r.n, f, 5)
+    old = A.get_dropin_options()
+    try:
+        A.set_dropin_options(A.options(precision=A.PREC_BF16, solver=A.SOLVER_CG))
+        X = A.do_als_with_csr(r.csr_ptr.astype(np.int32), r.csr_col, r.csr_val, th, r.m, r.n, f,
+                              0.05)
+    finally:
+        A.set_dropin_options(old)
+    th_r = torch.from_numpy(th).to(torch.bfloat16).float().numpy().astype(np.float64)
+    X_ref, _ = O.half_step(r.csr_ptr, r.csr_col, r.csr_val, th_r, 0.05)
+    keep = np.diff(r.csr_ptr) > 0
+    assert rel_rows(X, X_ref)[keep].max() < TOL
+    assert A.get_dropin_options().precision == A.PREC_FP32
