@@ -12,9 +12,9 @@
 //               box one row high, x = 0 and 64) into a 128B-swizzled MN-major
 //               tile (rows beyond the stage read TMA's zero fill); lanes 16-31
 //               write r_uk into the rating atom (column 128). Column indices
-//               and ratings of the next stage are loaded one stage ahead, item
-//               metadata two items ahead, so no dependent load is on the
-//               critical path.
+//               and ratings arrive DI - 1 stages ahead through a cp.async ring
+//               in shared memory, item metadata 32 items at a time, so no
+//               dependent global load is on the critical path.
 //   warp 9      MMA issuer (one thread): per stage, tcgen05.mma kind::f16,
 //               A = tile^T (M = 128: atoms 0, 1), B = tile (N = 144: atoms
 //               0, 1 and 16 columns of the rating atom), into one of two TMEM
@@ -56,6 +56,8 @@ constexpr int kN = 144;                           // MMA N: 128 theta columns + 
 constexpr int kBCol = 128;                        // D[:, 128] = b_u
 constexpr int kBufCols = 256;                     // TMEM columns per accumulator buffer
 constexpr int kTmemCols = 512;                    // two accumulators
+constexpr int DI = 8;                             // index-ring slots (stages fetched ahead + 1)
+constexpr int kRingSlot = 8 * KS + 32;            // column indices, ratings, two int4 of header
 }  // namespace ws
 
 struct WsGeom {
@@ -78,7 +80,10 @@ struct WsLayout {
   static constexpr size_t oCtrl = oSolver + 2 * kSolver;
   static constexpr size_t kBars = 8 * (2 * ws::NS + 10);  // 16-byte multiple
   static constexpr size_t kCtrl = kBars + 16 * (ws::NS + 2) + 16;
-  static constexpr size_t kTotal = 1024 + oCtrl + kCtrl;
+  static constexpr size_t oRing = oCtrl + kCtrl;  // 16-byte aligned
+  static constexpr size_t kTotal = 1024 + oRing + (size_t)ws::DI * ws::kRingSlot;
+  static_assert(kCtrl % 16 == 0 && ws::kRingSlot % 16 == 0, "ring alignment");
+  static_assert(kTotal <= 232448, "227 KB of shared memory per CTA");
 };
 
 struct WsCtrl {
@@ -111,62 +116,141 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
                : "memory");
 }
 
-__device__ __forceinline__ WorkItem load_item(const WsPlan &p, long long i) {
-  WorkItem w;
+// Work items are read a batch of 32 at a time (lane l holds the CTA's item
+// 32 * batch + l) and handed out with shuffles, so the next item's metadata
+// never waits on a load.
+struct ItemBatch {
+  int4 lo, hi;  // raw words of a WorkItem: {s, e}, {u, deg, part, heavy}
+};
+
+__device__ __forceinline__ ItemBatch load_batch(const WsPlan &p, long long bi, int lane) {
+  const long long i = blockIdx.x + (bi * 32 + lane) * (long long)gridDim.x;
+  ItemBatch b;
   if (i < p.nitems) {
-    w = p.items[i];
+    const int4 *q = reinterpret_cast<const int4 *>(p.items + i);
+    b.lo = q[0];
+    b.hi = q[1];
   } else {
-    w.s = w.e = 0;
-    w.u = -1;
-    w.deg = w.part = w.heavy = -1;
+    b.lo = make_int4(0, 0, 0, 0);
+    b.hi = make_int4(-1, -1, -1, -1);
   }
-  return w;
+  return b;
 }
 
-// Four column indices (lanes 0-15) or four ratings (lanes 16-31) of stage k0
-// of an item: rating slots 4q..4q+3 with q = lane mod 16. Slots past e give
-// the out-of-range row `oob` (TMA zero fill) / rating 0.
-__device__ __forceinline__ void load_quad(const RowsArgs &a, long long k0, long long e, int lane,
-                                          int oob, int (&cols)[4], float (&vals)[4]) {
-  const int q = lane & 15;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const long long k = k0 + 4 * q + j;
-    const bool in = k < e;
-    if (lane < 16) cols[j] = in ? a.col[k] : oob;
-    else vals[j] = in ? a.val[k] : 0.f;
-  }
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
 }
+
+// Fetch cursor of the producer warp: walks the CTA's items stage by stage,
+// ws::DI - 1 stages ahead of the stage being issued, and copies each stage's
+// column indices and ratings into a shared-memory ring with cp.async (one
+// commit group per stage). Rows without ratings are finished here (x_u = 0).
+template <typename LP>
+struct FetchCursor {
+  ItemBatch cb, nb;
+  long long bi;
+  int bpos;
+  long long s, e, k0;
+  int u, deg, part, heavy;
+
+  __device__ __forceinline__ void extract() {
+    s = ((long long)__shfl_sync(0xffffffffu, cb.lo.y, bpos) << 32) |
+        (unsigned)__shfl_sync(0xffffffffu, cb.lo.x, bpos);
+    e = ((long long)__shfl_sync(0xffffffffu, cb.lo.w, bpos) << 32) |
+        (unsigned)__shfl_sync(0xffffffffu, cb.lo.z, bpos);
+    u = __shfl_sync(0xffffffffu, cb.hi.x, bpos);
+    deg = __shfl_sync(0xffffffffu, cb.hi.y, bpos);
+    part = __shfl_sync(0xffffffffu, cb.hi.z, bpos);
+    heavy = __shfl_sync(0xffffffffu, cb.hi.w, bpos);
+  }
+  __device__ __forceinline__ void next_item(const WsPlan &p, int lane) {
+    if (++bpos == 32) {
+      cb = nb;
+      ++bi;
+      nb = load_batch(p, bi + 1, lane);
+      bpos = 0;
+    }
+    extract();
+  }
+  // advance to the next item with ratings, finishing empty rows on the way
+  __device__ __forceinline__ void settle(const RowsArgs &a, const WsPlan &p, int lane,
+                                         unsigned long long &n_empty) {
+    while (u >= 0 && e == s) {
+      for (int i = lane; i < a.f; i += 32) {
+        a.dst[(long long)u * a.ld_dst + i] = 0.f;
+        if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[(long long)u * a.ld_dst_lp + i] = LP(0.f);
+      }
+      if (lane == 0) {
+        if (a.row_flags) a.row_flags[u] = kRowEmpty;
+        ++n_empty;
+      }
+      next_item(p, lane);
+    }
+    k0 = s;
+  }
+  __device__ __forceinline__ void init(const RowsArgs &a, const WsPlan &p, int lane,
+                                       unsigned long long &n_empty) {
+    bi = 0;
+    bpos = 0;
+    cb = load_batch(p, 0, lane);
+    nb = load_batch(p, 1, lane);
+    extract();
+    settle(a, p, lane, n_empty);
+  }
+  // copies of stage `seq` into ring slot seq mod DI; an invalid header past the end
+  __device__ __forceinline__ void fetch(const RowsArgs &a, const WsPlan &p, unsigned char *ring,
+                                        long long seq, int lane, unsigned long long &n_empty) {
+    unsigned char *rs = ring + (int)(seq % ws::DI) * ws::kRingSlot;
+    if (u >= 0) {
+      const int kc = (int)(e - k0 < ws::KS ? e - k0 : ws::KS);
+      const uint32_t r0 = tc::smem_u32(rs);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int k = lane + 32 * j;
+        if (k < kc) {
+          cp_async4(r0 + 4 * k, a.col + k0 + k);
+          cp_async4(r0 + 4 * ws::KS + 4 * k, a.val + k0 + k);
+        }
+      }
+      if (lane == 0) {
+        int4 *h = reinterpret_cast<int4 *>(rs + 8 * ws::KS);
+        h[0] = make_int4(u, deg, part, heavy);
+        h[1] = make_int4(kc, k0 == s ? 1 : 0, k0 + ws::KS >= e ? 1 : 0, 1);
+      }
+      k0 += ws::KS;
+      if (k0 >= e) {
+        next_item(p, lane);
+        settle(a, p, lane, n_empty);
+      }
+    } else if (lane == 0) {
+      reinterpret_cast<int4 *>(rs + 8 * ws::KS)[1] = make_int4(0, 0, 0, 0);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+};
 
 template <typename LP>
 __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &g,
-                           const WsCtrl &c, unsigned char *stages, const void *tmap,
-                           unsigned long long &n_empty_rows) {
+                           const WsCtrl &c, unsigned char *stages, unsigned char *ring,
+                           const void *tmap, unsigned long long &n_empty_rows) {
   const int lane = threadIdx.x & 31;
   const uint32_t st0 = tc::smem_u32(stages);
-  const long long G = gridDim.x;
   unsigned empty_par = 0, empty_used = 0, row_par = 0, row_used = 0;
-  int slot = 0;
+  int slot = 0, b = 0;
   long long nrow = 0;
-  long long idx = blockIdx.x;
-  WorkItem cur = load_item(plan, idx), nxt = load_item(plan, idx + G);
-  int cols[4] = {0, 0, 0, 0};
-  float vals[4] = {0.f, 0.f, 0.f, 0.f};
-  if (cur.u >= 0) load_quad(a, cur.s, cur.e, lane, plan.src_rows, cols, vals);
-  while (cur.u >= 0 && !c.misc[1]) {
-    const WorkItem nn = load_item(plan, idx + 2 * G);  // metadata two items ahead
-    if (cur.e == cur.s) {  // a row without ratings: x_u = 0
-      for (int i = lane; i < a.f; i += 32) {
-        a.dst[(long long)cur.u * a.ld_dst + i] = 0.f;
-        if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[(long long)cur.u * a.ld_dst_lp + i] = LP(0.f);
-      }
-      if (lane == 0) {
-        if (a.row_flags) a.row_flags[cur.u] = kRowEmpty;
-        ++n_empty_rows;
-      }
-      if (nxt.u >= 0) load_quad(a, nxt.s, nxt.e, lane, plan.src_rows, cols, vals);
-    } else {
-      const int b = (int)(nrow & 1);
+  FetchCursor<LP> fc;
+  fc.init(a, plan, lane, n_empty_rows);
+  for (int q = 0; q < ws::DI - 1; ++q) fc.fetch(a, plan, ring, q, lane, n_empty_rows);
+  for (long long n = 0;; ++n) {
+    fc.fetch(a, plan, ring, n + ws::DI - 1, lane, n_empty_rows);
+    asm volatile("cp.async.wait_group %0;" ::"n"(ws::DI - 1) : "memory");
+    __syncwarp();
+    const unsigned char *rs = ring + (int)(n % ws::DI) * ws::kRingSlot;
+    const int4 h1 = reinterpret_cast<const int4 *>(rs + 8 * ws::KS)[1];
+    if (__any_sync(0xffffffffu, h1.w == 0 || c.misc[1] != 0)) break;  // warp-uniform exit
+    const int kc = h1.x, first = h1.y, last = h1.z;
+    if (first) {
+      b = (int)(nrow & 1);
       ++nrow;
       if (lane == 0) {
         bool okr = true;
@@ -176,70 +260,56 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
         }
         row_used |= 1u << b;
         if (!okr) c.misc[1] = 1;
-        c.row_info[b] = make_int4(cur.u, cur.deg, cur.part, cur.heavy);
+        c.row_info[b] = reinterpret_cast<const int4 *>(rs + 8 * ws::KS)[0];
         tc::mbar_arrive(&c.row_full[b]);
       }
-      const int nst = (int)((cur.e - cur.s + ws::KS - 1) / ws::KS);
-      for (int gi = 0; gi < nst; ++gi) {
-        const long long k0 = cur.s + (long long)gi * ws::KS;
-        const int kc = (int)(cur.e - k0 < ws::KS ? cur.e - k0 : ws::KS);
-        const int krows = (kc + 15) & ~15;
-        // indices of the next stage (this item's or the next item's first)
-        int ncols[4];
-        float nvals[4];
-        if (gi + 1 < nst) load_quad(a, k0 + ws::KS, cur.e, lane, plan.src_rows, ncols, nvals);
-        else if (nxt.u >= 0) load_quad(a, nxt.s, nxt.e, lane, plan.src_rows, ncols, nvals);
-        bool okw = true;
-        if (empty_used & (1u << slot)) {
-          okw = tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
-          empty_par ^= 1u << slot;
-        }
-        empty_used |= 1u << slot;
-        if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
-        const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
-        if (lane == 0) {
-          c.stage_info[slot] = make_int4(b, krows / 16, gi == 0 ? 1 : 0, gi == nst - 1 ? 1 : 0);
-          mbar_arrive_tx(&c.full[slot], (uint32_t)((krows / 4) * g.atoms * 512));
-        }
-        __syncwarp();
-        const int q = lane & 15;
-        if (lane < 16) {
-          if (4 * q < krows) {
-            const uint32_t dst = sa + (q >> 1) * 1024 + (q & 1) * 512;
-            tma_gather4(dst, tmap, 0, cols[0], cols[1], cols[2], cols[3], &c.full[slot]);
-            if (g.atoms > 1)
-              tma_gather4(dst + ws::kAtom, tmap, 64, cols[0], cols[1], cols[2], cols[3],
-                          &c.full[slot]);
-          }
-        } else {
+    }
+    const int krows = (kc + 15) & ~15;
+    bool okw = true;
+    if (empty_used & (1u << slot)) {
+      okw = tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
+      empty_par ^= 1u << slot;
+    }
+    empty_used |= 1u << slot;
+    if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
+    const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
+    if (lane == 0) {
+      c.stage_info[slot] = make_int4(b, krows / 16, first, last);
+      mbar_arrive_tx(&c.full[slot], (uint32_t)((krows / 4) * g.atoms * 512));
+    }
+    __syncwarp();
+    const int q = lane & 15;
+    if (lane < 16) {
+      if (4 * q < krows) {
+        const int4 cq = reinterpret_cast<const int4 *>(rs)[q];
+        const int oob = plan.src_rows;
+        const int c0 = 4 * q < kc ? cq.x : oob, c1 = 4 * q + 1 < kc ? cq.y : oob;
+        const int c2 = 4 * q + 2 < kc ? cq.z : oob, c3 = 4 * q + 3 < kc ? cq.w : oob;
+        const uint32_t dst = sa + (q >> 1) * 1024 + (q & 1) * 512;
+        tma_gather4(dst, tmap, 0, c0, c1, c2, c3, &c.full[slot]);
+        if (g.atoms > 1) tma_gather4(dst + ws::kAtom, tmap, 64, c0, c1, c2, c3, &c.full[slot]);
+      }
+    } else {
+      const float4 vq = reinterpret_cast<const float4 *>(rs + 4 * ws::KS)[q];
+      const float vv[4] = {vq.x, vq.y, vq.z, vq.w};
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int k = 4 * q + j;
-            if (k < krows) {
-              const uint32_t w0 = k < kc ? (uint32_t)tc::to_bits<LP>(vals[j]) : 0u;
-              const uint32_t dst = sa + 2 * ws::kAtom + (k >> 3) * 1024 + (k & 7) * 128 + ((k & 7) << 4);
-              asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(w0),
-                           "r"(0u), "r"(0u), "r"(0u)
-                           : "memory");
-            }
-          }
-          tc::fence_proxy_async();
-        }
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive(&c.full[slot]);  // releases the rating stores
-        slot = slot + 1 == ws::NS ? 0 : slot + 1;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          cols[j] = ncols[j];
-          vals[j] = nvals[j];
+      for (int j = 0; j < 4; ++j) {
+        const int k = 4 * q + j;
+        if (k < krows) {
+          const uint32_t w0 = k < kc ? (uint32_t)tc::to_bits<LP>(vv[j]) : 0u;
+          const uint32_t dst = sa + 2 * ws::kAtom + (k >> 3) * 1024 + (k & 7) * 128 + ((k & 7) << 4);
+          asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(w0), "r"(0u),
+                       "r"(0u), "r"(0u)
+                       : "memory");
         }
       }
-      if (c.misc[1]) break;
+      tc::fence_proxy_async();
     }
-    idx += G;
-    cur = nxt;
-    nxt = nn;
+    __syncwarp();
+    if (lane == 0) tc::mbar_arrive(&c.full[slot]);  // releases the rating stores
+    slot = slot + 1 == ws::NS ? 0 : slot + 1;
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into the ring outlives the warp
   // end marker for the MMA thread
   if (empty_used & (1u << slot))
     tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
@@ -248,11 +318,11 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     mbar_arrive_tx(&c.full[slot], 0);
     tc::mbar_arrive(&c.full[slot]);
     // end markers for both solver warpgroups
-    for (int b = 0; b < 2; ++b) {
-      if (row_used & (1u << b))
-        tc::mbar_wait_or_abort(&c.row_empty[b], (row_par >> b) & 1, c.misc + 1);
-      c.row_info[b] = make_int4(-1, 0, 0, 0);
-      tc::mbar_arrive(&c.row_full[b]);
+    for (int bb = 0; bb < 2; ++bb) {
+      if (row_used & (1u << bb))
+        tc::mbar_wait_or_abort(&c.row_empty[bb], (row_par >> bb) & 1, c.misc + 1);
+      c.row_info[bb] = make_int4(-1, 0, 0, 0);
+      tc::mbar_arrive(&c.row_full[bb]);
     }
   }
   __syncwarp();
@@ -655,7 +725,7 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan,
     if ((tid & 31) == 0) ws_mma(a, c, base, tmem, idesc);
     __syncwarp();
   } else if (warp == ws::kProdWarp) {
-    ws_produce<LP>(a, plan, g, c, base, &tmap, n_empty);
+    ws_produce<LP>(a, plan, g, c, base, base + L::oRing, &tmap, n_empty);
     if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
   } else if (warp < 8) {
     ws_solve<FP, NP, LP>(a, plan, sv, c, base + L::oSolver + (size_t)(warp >> 2) * L::kSolver,
