@@ -727,3 +727,79 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
   DROPIN_CALL(freeBest(csrRowIndex), "doALSWithCSR: free csrRowIndex");
   DROPIN_CALL(freeBest(csrColIndex), "doALSWithCSR: free csrColIndex");
 }
+
+// ---------------------------------------------------------------------------
+// als_half_step_static: the stand-alone FP32 half-step with its scratch (the
+// degree-binned visiting order, the row-queue head and the counters) in a
+// file-scope device array, so that a call allocates nothing.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kStaticQueueOff = (sizeof(int32_t) * (size_t)ALS_STATIC_MAX_ROWS + 255) / 256 * 256;
+constexpr size_t kStaticCtrOff =
+    kStaticQueueOff + (sizeof(unsigned) * (1 + 3 * (size_t)kOrderBins) + 255) / 256 * 256;
+constexpr size_t kStaticBytes = kStaticCtrOff + (sizeof(Counters) + 255) / 256 * 256;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+namespace {
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+void *g_static_ptr[kStaticMaxDevices];
+
+// Device address of the scratch array on the current device, looked up with
+// cudaGetSymbolAddress the first time a call runs on that device.
+int static_scratch(void **out) {
+  int dev = 0;
+  ALS_TRY(cudaGetDevice(&dev), "als_half_step_static: cudaGetDevice");
+  if (dev < 0 || dev >= kStaticMaxDevices)
+    return fail(ALS_ERR_UNSUPPORTED, "als_half_step_static: device ordinal above 63");
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void *p = nullptr;
+    ALS_TRY(cudaGetSymbolAddress(&p, g_static_scratch), "als_half_step_static: cudaGetSymbolAddress");
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return ALS_OK;
+}
+}  // namespace
+
+int als_half_step_static(int64_t m, int64_t n, int32_t f, const int64_t *ptr, const int32_t *col,
+                         const float *val, const float *src, int32_t ld_src, float *dst,
+                         int32_t ld_dst, float lambda, const als_options *opt, cudaStream_t st) {
+  if (m < 0 || n <= 0 || f <= 0) return fail(ALS_ERR_INVALID, "bad sizes");
+  if (m > ALS_STATIC_MAX_ROWS)
+    return fail(ALS_ERR_INVALID, "als_half_step_static: " + std::to_string(m) +
+                                     " rows exceed the static scratch limit of " +
+                                     std::to_string(ALS_STATIC_MAX_ROWS) +
+                                     " rows; use als_half_step with a caller workspace");
+  if (m == 0) return ALS_OK;
+  if (!ptr || !src || !dst || ld_src < f || ld_dst < f)
+    return fail(ALS_ERR_INVALID, "bad pointers or strides");
+  als_options o;
+  als_default_options(&o);
+  if (opt) o = *opt;
+  if (o.precision != ALS_PREC_FP32)
+    return fail(ALS_ERR_UNSUPPORTED, "als_half_step_static takes FP32 factors");
+  int rc = check_options(o, f);
+  if (rc != ALS_OK) return rc;
+  void *scratch = nullptr;
+  if ((rc = static_scratch(&scratch)) != ALS_OK) return rc;
+  char *b = static_cast<char *>(scratch);
+  int32_t *order = reinterpret_cast<int32_t *>(b);
+  unsigned *queue = reinterpret_cast<unsigned *>(b + kStaticQueueOff);
+  Counters *ctr = reinterpret_cast<Counters *>(b + kStaticCtrOff);
+  // Zeroed on every call: the counters and the row-queue head. The degree
+  // histogram behind queue + 1 is cleared by launch_degree_order itself, and
+  // every entry of the order it reads is written before it is read.
+  ALS_TRY(cudaMemsetAsync(ctr, 0, sizeof(Counters), st), "als_half_step_static: counters");
+  ALS_TRY(cudaMemsetAsync(queue, 0, sizeof(unsigned), st), "als_half_step_static: queue");
+  ALS_TRY(launch_degree_order(ptr, m, order, queue + 1, st), "als_half_step_static: degree order");
+  RowsArgs a{};
+  a.m = m; a.f = f; a.lambda = lambda; a.row_ptr = ptr; a.col = col; a.val = val;
+  a.src = src; a.ld_src = ld_src; a.dst = dst; a.ld_dst = ld_dst;
+  a.order = order; a.queue = queue; a.counters = ctr; a.refine_tol = o.refine_tol;
+  ALS_TRY(launch_rows_fp32(a, kLpNone, device_sm_count(), st), "als_half_step_static");
+  return ALS_OK;
+}

@@ -176,6 +176,20 @@ int als_half_step(int64_t m, int64_t n, int32_t f, const int64_t *d_row_ptr,
                   float *d_dst, int32_t ld_dst, float lambda, const als_options *opt,
                   void *d_work, size_t work_bytes, cudaStream_t stream);
 
+/* The same FP32 half-step without a workspace argument: its scratch (visiting
+ * order, row queue, counters) is a file-scope __device__ array sized for at
+ * most ALS_STATIC_MAX_ROWS rows (about 4 MiB), so a call allocates nothing.
+ * Larger m is rejected with ALS_ERR_INVALID. The first call on each device
+ * looks the array up with cudaGetSymbolAddress; make that first call before
+ * any stream capture. Calls that overlap in time (two streams, two host
+ * threads) share the one array and race: serialise them.
+ * No counterpart in the reference. */
+#define ALS_STATIC_MAX_ROWS 1048576
+int als_half_step_static(int64_t m, int64_t n, int32_t f, const int64_t *d_row_ptr,
+                         const int32_t *d_col, const float *d_val, const float *d_src,
+                         int32_t ld_src, float *d_dst, int32_t ld_dst, float lambda,
+                         const als_options *opt, cudaStream_t stream);
+
 /* RMSE / predict over COO triplets with caller factors. */
 size_t als_rmse_work_bytes(void);
 int als_rmse(int64_t nt, const int32_t *d_u, const int32_t *d_i, const float *d_r,
