@@ -58,7 +58,7 @@ class Options(ctypes.Structure):
                 ("cg_max_steps", c_i32), ("cg_tol", c_f32), ("refine_tol", c_f32),
                 ("use_graph", c_i32), ("mlp_train_iters", c_i32), ("mlp_steps", c_i32),
                 ("mlp_batch", c_i32), ("mlp_lr", c_f32), ("cg_jacobi", c_i32),
-                ("reserved", c_i32 * 4)]
+                ("solver_groups", c_i32), ("reserved", c_i32 * 3)]
 
 
 class Stats(ctypes.Structure):

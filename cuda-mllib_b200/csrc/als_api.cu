@@ -56,6 +56,7 @@ int check_options(const als_options &o, int f) {
     return fail(ALS_ERR_UNSUPPORTED, "tensor-core form supports rank f in 16..128");
   }
   if (o.cg_max_steps < 0 || o.cg_max_steps > 256) return fail(ALS_ERR_INVALID, "cg_max_steps");
+  if (o.solver_groups < 0 || o.solver_groups > 2) return fail(ALS_ERR_INVALID, "solver_groups must be 0, 1 or 2");
   if (o.warm_start < ALS_WARM_ZERO || o.warm_start > ALS_WARM_MLP)
     return fail(ALS_ERR_INVALID, "unknown warm start");
   if (o.warm_start == ALS_WARM_MLP &&
@@ -113,8 +114,8 @@ cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, c
   }
   a.src = src_lp;
   a.ld_src = ld_lp;
-  return launch_rows_tc(a, kind, o.solver, o.cg_max_steps, o.cg_tol, o.cg_jacobi, x0,
-                        s.has_plan ? &s.plan : nullptr, num_sms, st);
+  return launch_rows_tc(a, kind, o.solver, o.cg_max_steps, o.cg_tol, o.cg_jacobi,
+                        o.solver_groups, x0, s.has_plan ? &s.plan : nullptr, num_sms, st);
 }
 
 }  // namespace
@@ -160,6 +161,7 @@ void als_default_options(als_options *o) {
   o->mlp_batch = 8192;
   o->mlp_lr = 2e-3f;
   o->cg_jacobi = 0;
+  o->solver_groups = 0;
 }
 
 const char *als_last_error(void) { return g_last_error.c_str(); }

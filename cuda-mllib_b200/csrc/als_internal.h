@@ -20,8 +20,8 @@ bool tc_supported(int f);
 int tc_padded_ld(int f);  // row stride (elements) of the low-precision factor copy
 struct WsPlan;
 cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
-                           float cg_tol, int cg_jacobi, const float *x0, const WsPlan *plan,
-                           int num_sms, cudaStream_t st);
+                           float cg_tol, int cg_jacobi, int groups, const float *x0,
+                           const WsPlan *plan, int num_sms, cudaStream_t st);
 
 // Solver parameters of one launch.
 struct TcSolve {
@@ -31,6 +31,7 @@ struct TcSolve {
   const float *x0;     // CG starting point (m x ld_x0), or null for zero
   int ld_x0;
   int jacobi;          // 1: diagonal preconditioner
+  int groups;          // solver warpgroups per CTA of the warp-specialised kernel (1 or 2)
 };
 
 // Work list of the warp-specialised kernel, planned on the host per side:

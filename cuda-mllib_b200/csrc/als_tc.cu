@@ -388,12 +388,12 @@ static cudaError_t launch_tc_np(const RowsArgs &a, int lp_kind, const TcSolve &s
 }
 
 cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
-                           float cg_tol, int cg_jacobi, const float *x0, const WsPlan *plan,
-                           int num_sms, cudaStream_t st) {
+                           float cg_tol, int cg_jacobi, int groups, const float *x0,
+                           const WsPlan *plan, int num_sms, cudaStream_t st) {
   if (!tc_supported(a.f)) return cudaErrorNotSupported;
   if (a.ld_src != tc_padded_ld(a.f) || !a.error) return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
-  TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst, cg_jacobi};
+  TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst, cg_jacobi, groups == 1 ? 1 : 2};
   if (plan && tc_ws_supported(a.f)) return launch_rows_tc_ws(a, lp_kind, sv, *plan, num_sms, st);
   const int f = a.f, np = tc_geom(f).np;
   // (FP, NP): FP >= f is the Cholesky tile extent, NP = roundup16(f + 1) the MMA N

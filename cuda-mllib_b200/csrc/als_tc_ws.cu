@@ -7,14 +7,16 @@
 // global slots; the chunk that finishes last sums them in chunk order and
 // solves the row.
 //
-//   warp 8      producer: per stage of 64 ratings, lanes 0-15 issue TMA
-//               tile::gather4 loads (4 factor rows x 128 B per instruction,
-//               box one row high, x = 0 and 64) into a 128B-swizzled MN-major
-//               tile (rows beyond the stage read TMA's zero fill); lanes 16-31
-//               write r_uk into the rating atom (column 128). Column indices
-//               and ratings arrive DI - 1 stages ahead through a cp.async ring
-//               in shared memory, item metadata 32 items at a time, so no
-//               dependent global load is on the critical path.
+//   warp 8      producer: per stage of 64 ratings, 16-byte cp.async copies of
+//               the rated factor rows (half a warp per row, one 16-byte piece
+//               per lane) into a 128B-swizzled MN-major tile, the swizzle
+//               computed in the destination address; rows past the stage are
+//               zero-filled. The lanes also write r_uk into the rating atom
+//               (column 128). Completion reaches the MMA thread through
+//               cp.async.mbarrier.arrive. Column indices and ratings arrive
+//               DI - 1 stages ahead through a cp.async ring in shared memory,
+//               item metadata 32 items at a time, so no dependent global load
+//               is on the critical path.
 //   warp 9      MMA issuer (one thread): per stage, tcgen05.mma kind::f16,
 //               A = tile^T (M = 128: atoms 0, 1), B = tile (N = 144: atoms
 //               0, 1 and 16 columns of the rating atom), into one of two TMEM
@@ -27,11 +29,9 @@
 //               it, then CG in registers (optionally Jacobi-preconditioned;
 //               Cholesky fallback) or the register-tile Cholesky + FP64-residual
 //               refinement, each on its own named barrier.
-//   warps 10-11 idle (they only join the final barrier).
 //
 // Every mbarrier wait is bounded and gives up when another role aborted; a
 // timeout sets the error word and all roles leave their loops.
-#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -45,9 +45,12 @@
 namespace als {
 
 namespace ws {
-constexpr int kThreads = 384;
-constexpr int kProdWarp = 8;
-constexpr int kMmaWarp = 9;
+// NG solver warpgroups (warps 0 .. 4 NG - 1), then the producer and MMA warps.
+// With NG = 2 an SM sub-partition holds three warps, which caps a thread at
+// 168 registers; NG = 1 leaves two per sub-partition (up to 255).
+template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG + 64; }
+template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }
+template <int NG> __host__ __device__ constexpr int mma_warp() { return 4 * NG + 1; }
 constexpr int NS = 4;                             // shared-memory stages
 constexpr int KS = 64;                            // ratings per stage
 constexpr int kAtom = (KS / 8) * 1024;            // one 64-element MN atom of a stage
@@ -56,15 +59,16 @@ constexpr int kN = 144;                           // MMA N: 128 theta columns + 
 constexpr int kBCol = 128;                        // D[:, 128] = b_u
 constexpr int kBufCols = 256;                     // TMEM columns per accumulator buffer
 constexpr int kTmemCols = 512;                    // two accumulators
+constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
 constexpr int DI = 8;                             // index-ring slots (stages fetched ahead + 1)
 constexpr int kRingSlot = 8 * KS + 32;            // column indices, ratings, two int4 of header
 }  // namespace ws
 
 struct WsGeom {
-  int atoms;  // theta atoms loaded per stage: 1 when the factor rows fit 64 columns, else 2
+  int nj;  // 16-byte pieces per factor row (ld_src / 8, at most 16)
 };
 
-template <int FP, int NP>
+template <int FP, int NP, int NG>
 struct WsLayout {
   static constexpr int LDS = FP + 1;
   static constexpr size_t kS = (size_t)FP * LDS * 4;
@@ -77,7 +81,7 @@ struct WsLayout {
   static constexpr size_t oMisc = oRd + (size_t)FP * 8;
   static constexpr size_t kSolver = (oMisc + 16 + 127) / 128 * 128;
   static constexpr size_t oSolver = (size_t)ws::NS * ws::kStageBytes;
-  static constexpr size_t oCtrl = oSolver + 2 * kSolver;
+  static constexpr size_t oCtrl = oSolver + NG * kSolver;
   static constexpr size_t kBars = 8 * (2 * ws::NS + 10);  // 16-byte multiple
   static constexpr size_t kCtrl = kBars + 16 * (ws::NS + 2) + 16;
   static constexpr size_t oRing = oCtrl + kCtrl;  // 16-byte aligned
@@ -100,19 +104,18 @@ __device__ __forceinline__ void ws_abort(const RowsArgs &a, const WsCtrl &c) {
 // ---------------------------------------------------------------------------
 // producer warp
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void tma_gather4(uint32_t dst, const void *tmap, int x, int y0, int y1,
-                                            int y2, int y3, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3),
-      "r"(tc::smem_u32(bar))
-      : "memory");
+// No memory clobber: the copies are ordered by the mbarrier operations (all
+// asm volatile) around them, and the column indices feeding a run of copies
+// can be loaded ahead of it.
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async16_nc(uint32_t dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src));
 }
 
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)),
-               "r"(bytes)
+__device__ __forceinline__ void mbar_arrive_cnt(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(count)
                : "memory");
 }
 
@@ -229,10 +232,57 @@ struct FetchCursor {
   }
 };
 
+// One stage's factor rows: lanes 16h + j copy 16-byte piece j (< nj = ld / 8)
+// of rows k = 32h .. 32h + 31 (< krows) into the 128B-swizzled MN-major tile
+// (piece j of row k lands in atom j / 8, 8-row group k / 8, row k mod 8,
+// 16-byte chunk (j mod 8) xor (k mod 8)). Rows at or past kc are zero-filled;
+// a column index outside the factor matrix is clamped to its last row, so a
+// malformed CSR gives wrong numbers but never reads outside the factors. The
+// 32 column indices are read first, so the copies issue back to back.
+__device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &plan, int nj,
+                                             const int *cols, int kc, int krows, uint32_t sa,
+                                             int lane) {
+  const int j = lane & 15, k0 = (lane >> 4) * 32;
+  if (j >= nj || k0 >= krows) return;
+  int ci[32];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int4 v = reinterpret_cast<const int4 *>(cols + k0)[q];
+    ci[4 * q] = v.x;
+    ci[4 * q + 1] = v.y;
+    ci[4 * q + 2] = v.z;
+    ci[4 * q + 3] = v.w;
+  }
+  const char *srcb = reinterpret_cast<const char *>(a.src) + 16 * j;
+  const unsigned row_bytes = (unsigned)a.ld_src * 2u, last = (unsigned)plan.src_rows - 1u;
+  const uint32_t dj = sa + (uint32_t)(j >> 3) * ws::kAtom + (uint32_t)(k0 >> 3) * 1024;
+  const uint32_t jx = (uint32_t)(j & 7) << 4;
+  if (kc >= k0 + 32) {  // every row of this half carries a rating
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const unsigned c = min((unsigned)ci[i], last);
+      const uint32_t dst = dj + (uint32_t)((i >> 3) * 1024 + (i & 7) * 128) + (jx ^ ((uint32_t)(i & 7) << 4));
+      cp_async16_nc(dst, srcb + (size_t)c * row_bytes);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int k = k0 + i;
+      if (k < krows) {
+        const bool in = k < kc;
+        const unsigned c = min((unsigned)ci[i], last);
+        const char *src = in ? srcb + (size_t)c * row_bytes : srcb;
+        const uint32_t dst = dj + (uint32_t)((i >> 3) * 1024 + (i & 7) * 128) + (jx ^ ((uint32_t)(i & 7) << 4));
+        cp_async16_zfill(dst, src, in ? 16u : 0u);
+      }
+    }
+  }
+}
+
 template <typename LP>
 __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &g,
                            const WsCtrl &c, unsigned char *stages, unsigned char *ring,
-                           const void *tmap, unsigned long long &n_empty_rows) {
+                           unsigned long long &n_empty_rows) {
   const int lane = threadIdx.x & 31;
   const uint32_t st0 = tc::smem_u32(stages);
   unsigned empty_par = 0, empty_used = 0, row_par = 0, row_used = 0;
@@ -273,38 +323,17 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     empty_used |= 1u << slot;
     if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
     const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
-    if (lane == 0) {
-      c.stage_info[slot] = make_int4(b, krows / 16, first, last);
-      mbar_arrive_tx(&c.full[slot], (uint32_t)((krows / 4) * g.atoms * 512));
+    if (lane == 0) c.stage_info[slot] = make_int4(b, krows / 16, first, last);
+    gather_stage(a, plan, g.nj, reinterpret_cast<const int *>(rs), kc, krows, sa, lane);
+    // r_uk (0 past kc) into column 0 of the rating atom; the rest of the atom stays zero
+    const float *vr = reinterpret_cast<const float *>(rs + 4 * ws::KS);
+    for (int k = lane; k < krows; k += 32) {
+      const uint16_t w = k < kc ? tc::to_bits<LP>(vr[k]) : (uint16_t)0;
+      const uint32_t dst = sa + 2 * ws::kAtom + (k >> 3) * 1024 + (k & 7) * 128 + ((k & 7) << 4);
+      asm volatile("st.shared.u16 [%0], %1;" ::"r"(dst), "h"(w));
     }
-    __syncwarp();
-    const int q = lane & 15;
-    if (lane < 16) {
-      if (4 * q < krows) {
-        const int4 cq = reinterpret_cast<const int4 *>(rs)[q];
-        const int oob = plan.src_rows;
-        const int c0 = 4 * q < kc ? cq.x : oob, c1 = 4 * q + 1 < kc ? cq.y : oob;
-        const int c2 = 4 * q + 2 < kc ? cq.z : oob, c3 = 4 * q + 3 < kc ? cq.w : oob;
-        const uint32_t dst = sa + (q >> 1) * 1024 + (q & 1) * 512;
-        tma_gather4(dst, tmap, 0, c0, c1, c2, c3, &c.full[slot]);
-        if (g.atoms > 1) tma_gather4(dst + ws::kAtom, tmap, 64, c0, c1, c2, c3, &c.full[slot]);
-      }
-    } else {
-      const float4 vq = reinterpret_cast<const float4 *>(rs + 4 * ws::KS)[q];
-      const float vv[4] = {vq.x, vq.y, vq.z, vq.w};
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = 4 * q + j;
-        if (k < krows) {
-          const uint32_t w0 = k < kc ? (uint32_t)tc::to_bits<LP>(vv[j]) : 0u;
-          const uint32_t dst = sa + 2 * ws::kAtom + (k >> 3) * 1024 + (k & 7) * 128 + ((k & 7) << 4);
-          asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(w0), "r"(0u),
-                       "r"(0u), "r"(0u)
-                       : "memory");
-        }
-      }
-      tc::fence_proxy_async();
-    }
+    tc::fence_proxy_async();             // the rating stores, for the tensor core
+    tc::cp_async_arrive(&c.full[slot]);  // once this lane's copies have landed
     __syncwarp();
     if (lane == 0) tc::mbar_arrive(&c.full[slot]);  // releases the rating stores
     slot = slot + 1 == ws::NS ? 0 : slot + 1;
@@ -315,8 +344,7 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
   if (lane == 0) {
     c.stage_info[slot] = make_int4(-1, 0, 0, 0);
-    mbar_arrive_tx(&c.full[slot], 0);
-    tc::mbar_arrive(&c.full[slot]);
+    mbar_arrive_cnt(&c.full[slot], ws::kFullCount);
     // end markers for both solver warpgroups
     for (int bb = 0; bb < 2; ++bb) {
       if (row_used & (1u << bb))
@@ -474,10 +502,13 @@ __device__ __noinline__ int ws_cholesky(float *S, float *dg, float *bv, float *x
   return refined ? 2 : 0;
 }
 
-template <int FP, int NP, typename LP>
+// Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA; row n
+// sits in accumulator n mod 2 (with NG = 2 each group keeps one accumulator,
+// with NG = 1 the group alternates between both).
+template <int FP, int NP, typename LP, int NG>
 __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &sv,
                          const WsCtrl &c, unsigned char *mem, uint32_t tmem, int wg) {
-  using L = WsLayout<FP, NP>;
+  using L = WsLayout<FP, NP, NG>;
   constexpr int LDS = L::LDS, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
   static_assert(NTILES <= 128, "one warpgroup holds at most 128 Cholesky tiles");
   const int lt = threadIdx.x & 127, wl = (threadIdx.x >> 5) & 3;
@@ -492,22 +523,24 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   const bool live = m < f;
   ps[lt] = 0.f;  // L::kPs == 128 entries, one per thread
   B.sync();
-  unsigned par = 0;
+  unsigned parb = 0;  // phase parity per accumulator
   int rslot = 0;
   unsigned long long n_rows = 0, n_ref = 0, n_bad = 0, n_steps = 0, n_fb = 0, n_r0 = 0;
-  const uint32_t tbase = tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)wg * ws::kBufCols;
-  for (;;) {
-    bool ok = tc::mbar_wait_or_abort(&c.row_full[wg], par, c.misc + 1);
+  const uint32_t tlane = tmem + ((uint32_t)(wl * 32) << 16);
+  for (int b = wg;; b = NG == 1 ? b ^ 1 : b) {
+    const unsigned par = (parb >> b) & 1u;
+    const uint32_t tbase = tlane + (uint32_t)b * ws::kBufCols;
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[b], par, c.misc + 1);
     if (!B.all(ok)) { ws_abort(a, c); break; }
-    const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[wg]);
+    const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[b]);
     const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
     B.sync();
-    if (lt == 0) tc::mbar_arrive(&c.row_empty[wg]);
+    if (lt == 0) tc::mbar_arrive(&c.row_empty[b]);
     if (info.x < 0) break;
     const int64_t u = info.x;
     const float reg = a.lambda * (float)info.y;
-    ok = tc::mbar_wait_or_abort(&c.acc_full[wg], par, c.misc + 1);
-    par ^= 1;
+    ok = tc::mbar_wait_or_abort(&c.acc_full[b], par, c.misc + 1);
+    parb ^= 1u << b;
     if (!B.all(ok)) { ws_abort(a, c); break; }
     tc::tc_fence_after();
     // Thread m <- row m of D. Columns >= f and rows >= f of D are zero (zero
@@ -527,7 +560,7 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       bm = v[0];
     }
     tc::tc_fence_before();
-    tc::mbar_arrive(&c.acc_empty[wg]);  // the accumulator may be overwritten now
+    tc::mbar_arrive(&c.acc_empty[b]);  // the accumulator may be overwritten now
     if (info.z >= 0) {
       // A chunk of a split row: store the partial sums; the chunk that
       // finishes last adds all of them, in chunk order, and solves the row.
@@ -670,11 +703,10 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   }
 }
 
-template <int FP, int NP, typename LP>
-__global__ void __launch_bounds__(ws::kThreads, 1)
-rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan,
-                  const __grid_constant__ CUtensorMap tmap) {
-  using L = WsLayout<FP, NP>;
+template <int FP, int NP, typename LP, int NG>
+__global__ void __launch_bounds__(ws::threads<NG>(), 1)
+rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan) {
+  using L = WsLayout<FP, NP, NG>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char *base = smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023);
   unsigned char *ctrl = base + L::oCtrl;
@@ -693,7 +725,7 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan,
 
   if (tid == 0) {
     for (int i = 0; i < ws::NS; ++i) {
-      tc::mbar_init(&c.full[i], 2);  // expect-tx arrive + the arrive releasing the rating stores
+      tc::mbar_init(&c.full[i], ws::kFullCount);
       tc::mbar_init(&c.empty[i], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -706,13 +738,13 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan,
     c.misc[1] = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == ws::kMmaWarp) {
+  if (warp == ws::mma_warp<NG>()) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      tc::smem_u32((const void *)&c.misc[0])),
                  "r"(ws::kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  for (int q = tid; q < ws::NS * ws::kStageBytes / 16; q += ws::kThreads)
+  for (int q = tid; q < ws::NS * ws::kStageBytes / 16; q += ws::threads<NG>())
     reinterpret_cast<uint4 *>(base)[q] = make_uint4(0, 0, 0, 0);
   tc::fence_proxy_async();
   tc::tc_fence_before();
@@ -721,19 +753,19 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan,
   const uint32_t tmem = (uint32_t)c.misc[0];
   unsigned long long n_empty = 0;
 
-  if (warp == ws::kMmaWarp) {
+  if (warp == ws::mma_warp<NG>()) {
     if ((tid & 31) == 0) ws_mma(a, c, base, tmem, idesc);
     __syncwarp();
-  } else if (warp == ws::kProdWarp) {
-    ws_produce<LP>(a, plan, g, c, base, base + L::oRing, &tmap, n_empty);
+  } else if (warp == ws::prod_warp<NG>()) {
+    ws_produce<LP>(a, plan, g, c, base, base + L::oRing, n_empty);
     if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
-  } else if (warp < 8) {
-    ws_solve<FP, NP, LP>(a, plan, sv, c, base + L::oSolver + (size_t)(warp >> 2) * L::kSolver,
-                         tmem, warp >> 2);
+  } else if (warp < 4 * NG) {
+    ws_solve<FP, NP, LP, NG>(a, plan, sv, c, base + L::oSolver + (size_t)(warp >> 2) * L::kSolver,
+                             tmem, warp >> 2);
   }
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == ws::kMmaWarp) {
+  if (warp == ws::mma_warp<NG>()) {
     tc::tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(ws::kTmemCols));
@@ -743,62 +775,33 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan,
 bool tc_ws_supported(int f) { return f >= 16 && f <= 112; }
 int tc_ws_np(int f) { return ((f + 15) / 16) * 16; }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static cudaError_t encode_rows_map(CUtensorMap *map, const void *src, int rows, int ldp,
-                                   int lp_kind) {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
-    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return cudaErrorNotSupported;
-    fn = (EncodeTiledFn)p;
-  }
-  // rows x ldp elements (16-bit), row stride 2*ldp bytes; box 64 x 1 (gather4 loads 4 rows)
-  const cuuint64_t dims[2] = {(cuuint64_t)ldp, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)ldp * 2};
-  const cuuint32_t box[2] = {64, 1};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = fn(map, lp_kind == kLpBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
-                        2, const_cast<void *>(src), dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
-}
-
-template <int FP, int NP, typename LP>
+template <int FP, int NP, typename LP, int NG>
 static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
                              const WsPlan &plan, int num_sms, cudaStream_t st) {
-  using L = WsLayout<FP, NP>;
+  using L = WsLayout<FP, NP, NG>;
   WsGeom g;
-  g.atoms = a.ld_src <= 64 ? 1 : 2;
+  g.nj = a.ld_src / 8;
   if (a.ld_src % 8 != 0 || a.ld_src > 128 || NP < a.f || FP < a.f || plan.part_ld < NP + 1)
     return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
-  CUtensorMap map;
-  cudaError_t err = encode_rows_map(&map, a.src, plan.src_rows, a.ld_src, lp_kind);
-  if (err != cudaSuccess) return err;
-  auto kern = rows_tc_ws_kernel<FP, NP, LP>;
-  err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kTotal);
+  auto kern = rows_tc_ws_kernel<FP, NP, LP, NG>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kTotal);
   if (err != cudaSuccess) return err;
   int64_t grid = num_sms;
   if (grid > plan.nitems) grid = plan.nitems > 0 ? plan.nitems : 1;
   const uint32_t idesc = tc::make_idesc(lp_kind == kLpBf16 ? 1 : 0, ws::kN);
-  kern<<<(unsigned)grid, ws::kThreads, L::kTotal, st>>>(a, idesc, sv, g, plan, map);
+  kern<<<(unsigned)grid, ws::threads<NG>(), L::kTotal, st>>>(a, idesc, sv, g, plan);
   return cudaGetLastError();
 }
 
 template <int FP, int NP>
 static cudaError_t launch_ws_np(const RowsArgs &a, int lp_kind, const TcSolve &sv,
                                 const WsPlan &plan, int num_sms, cudaStream_t st) {
-  return lp_kind == kLpBf16 ? launch_ws<FP, NP, __nv_bfloat16>(a, lp_kind, sv, plan, num_sms, st)
-                            : launch_ws<FP, NP, __half>(a, lp_kind, sv, plan, num_sms, st);
+  if (sv.groups == 1)
+    return lp_kind == kLpBf16 ? launch_ws<FP, NP, __nv_bfloat16, 1>(a, lp_kind, sv, plan, num_sms, st)
+                              : launch_ws<FP, NP, __half, 1>(a, lp_kind, sv, plan, num_sms, st);
+  return lp_kind == kLpBf16 ? launch_ws<FP, NP, __nv_bfloat16, 2>(a, lp_kind, sv, plan, num_sms, st)
+                            : launch_ws<FP, NP, __half, 2>(a, lp_kind, sv, plan, num_sms, st);
 }
 
 // f in [16, 112]: NP = roundup16(f) accumulator columns are read back per row,

@@ -95,7 +95,9 @@ typedef struct als_options {
   float mlp_lr;            /* Adam learning rate (default 2e-3)                   */
   int32_t cg_jacobi;       /* 1: diagonal (Jacobi) preconditioner for CG (default 0:
                               it slowed convergence on the benchmark matrices) */
-  int32_t reserved[4];
+  int32_t solver_groups;   /* solver warpgroups per SM in the tensor-core kernel:
+                              0 = chosen by the engine, 1 or 2                   */
+  int32_t reserved[3];
 } als_options;
 
 typedef struct als_stats {
