@@ -11,19 +11,20 @@
 //               the rated factor rows (half a warp per row, one 16-byte piece
 //               per lane) into a 128B-swizzled MN-major tile, the swizzle
 //               computed in the destination address; rows past the stage are
-//               zero-filled. The lanes also write r_uk into the rating atom
-//               (column 128). Completion reaches the MMA thread through
+//               zero-filled. The lanes also write r_uk into tile column
+//               c_r = ld (a pad column the copies never touch). Completion
+//               reaches the MMA thread through
 //               cp.async.mbarrier.arrive. Column indices and ratings arrive
 //               DI - 1 stages ahead through a cp.async ring in shared memory,
 //               item metadata 32 items at a time, so no dependent global load
 //               is on the critical path.
 //   warp 9      MMA issuer (one thread): per stage, tcgen05.mma kind::f16,
-//               A = tile^T (M = 128: atoms 0, 1), B = tile (N = 144: atoms
-//               0, 1 and 16 columns of the rating atom), into one of two TMEM
-//               accumulators (rows alternate); tcgen05.commit frees the stage
-//               and, after the item's last stage, marks the accumulator full.
-//               D[:, :f] = sum theta theta^T, D[:, 128] = b_u; rows and columns
-//               f..127 stay zero.
+//               A = tile^T (M = 128), B = the first N = roundup16(max(NP,
+//               c_r + 1)) tile columns, into one of two TMEM accumulators
+//               (rows alternate); tcgen05.commit frees the stage and, after
+//               the item's last stage, marks the accumulator full.
+//               D[:f, :f] = sum theta theta^T, D[:f, c_r] = b_u; the other
+//               columns below c_r are zero, rows >= f are ignored.
 //   warps 0-3,  two solver warpgroups, one per accumulator: read D with
 //   4-7         tcgen05.ld (thread m <- TMEM lane m = row m of A_u), release
 //               it, then CG in registers (optionally Jacobi-preconditioned;
@@ -51,14 +52,13 @@ namespace ws {
 template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG + 64; }
 template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }
 template <int NG> __host__ __device__ constexpr int mma_warp() { return 4 * NG + 1; }
-constexpr int NS = 4;                             // shared-memory stages
+constexpr int NS = 6;                             // shared-memory stages
 constexpr int KS = 64;                            // ratings per stage
 constexpr int kAtom = (KS / 8) * 1024;            // one 64-element MN atom of a stage
-constexpr int kStageBytes = 3 * kAtom;            // theta atoms 0, 1 and the rating atom
-constexpr int kN = 144;                           // MMA N: 128 theta columns + 16 (rating)
-constexpr int kBCol = 128;                        // D[:, 128] = b_u
-constexpr int kBufCols = 256;                     // TMEM columns per accumulator buffer
-constexpr int kTmemCols = 512;                    // two accumulators
+constexpr int kStageBytes = 2 * kAtom;            // tile columns 0-63 and 64-127
+constexpr int kAcc = 4;                           // TMEM accumulators (row n -> n mod 4)
+constexpr int kBufCols = 128;                     // TMEM columns per accumulator
+constexpr int kTmemCols = kAcc * kBufCols;        // all 512 columns
 constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
 constexpr int DI = 8;                             // index-ring slots (stages fetched ahead + 1)
 constexpr int kRingSlot = 8 * KS + 32;            // column indices, ratings, two int4 of header
@@ -82,7 +82,9 @@ struct WsLayout {
   static constexpr size_t kSolver = (oMisc + 16 + 127) / 128 * 128;
   static constexpr size_t oSolver = (size_t)ws::NS * ws::kStageBytes;
   static constexpr size_t oCtrl = oSolver + NG * kSolver;
-  static constexpr size_t kBars = 8 * (2 * ws::NS + 10);  // 16-byte multiple
+  // full, empty per stage; acc_full, acc_empty per accumulator; row_full,
+  // row_empty per row slot; drain; one spare (16-byte multiple)
+  static constexpr size_t kBars = 8 * (2 * ws::NS + 2 * ws::kAcc + 6);
   static constexpr size_t kCtrl = kBars + 16 * (ws::NS + 2) + 16;
   static constexpr size_t oRing = oCtrl + kCtrl;  // 16-byte aligned
   static constexpr size_t kTotal = 1024 + oRing + (size_t)ws::DI * ws::kRingSlot;
@@ -286,7 +288,7 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
   const int lane = threadIdx.x & 31;
   const uint32_t st0 = tc::smem_u32(stages);
   unsigned empty_par = 0, empty_used = 0, row_par = 0, row_used = 0;
-  int slot = 0, b = 0;
+  int slot = 0, acc = 0;
   long long nrow = 0;
   FetchCursor<LP> fc;
   fc.init(a, plan, lane, n_empty_rows);
@@ -300,7 +302,10 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     if (__any_sync(0xffffffffu, h1.w == 0 || c.misc[1] != 0)) break;  // warp-uniform exit
     const int kc = h1.x, first = h1.y, last = h1.z;
     if (first) {
-      b = (int)(nrow & 1);
+      // row nrow: row slot nrow mod 2 for the solver handshake, accumulator
+      // nrow mod kAcc for the MMA
+      const int b = (int)(nrow & 1);
+      acc = (int)(nrow & (ws::kAcc - 1));
       ++nrow;
       if (lane == 0) {
         bool okr = true;
@@ -323,13 +328,16 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     empty_used |= 1u << slot;
     if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
     const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
-    if (lane == 0) c.stage_info[slot] = make_int4(b, krows / 16, first, last);
+    if (lane == 0) c.stage_info[slot] = make_int4(acc, krows / 16, first, last);
     gather_stage(a, plan, g.nj, reinterpret_cast<const int *>(rs), kc, krows, sa, lane);
-    // r_uk (0 past kc) into column 0 of the rating atom; the rest of the atom stays zero
+    // r_uk (0 past kc) into tile column c_r = 8 nj: atom c_r / 64, 16-byte
+    // chunk ((c_r mod 64) / 8) xor (k mod 8), element 0; the chunk's other
+    // elements stay zero
     const float *vr = reinterpret_cast<const float *>(rs + 4 * ws::KS);
+    const uint32_t rbase = sa + (uint32_t)(g.nj >> 3) * ws::kAtom, rch = (uint32_t)(g.nj & 7);
     for (int k = lane; k < krows; k += 32) {
       const uint16_t w = k < kc ? tc::to_bits<LP>(vr[k]) : (uint16_t)0;
-      const uint32_t dst = sa + 2 * ws::kAtom + (k >> 3) * 1024 + (k & 7) * 128 + ((k & 7) << 4);
+      const uint32_t dst = rbase + (k >> 3) * 1024 + (k & 7) * 128 + ((rch ^ (uint32_t)(k & 7)) << 4);
       asm volatile("st.shared.u16 [%0], %1;" ::"r"(dst), "h"(w));
     }
     tc::fence_proxy_async();             // the rating stores, for the tensor core
@@ -402,19 +410,27 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
 // ---------------------------------------------------------------------------
 // solver warpgroup
 // ---------------------------------------------------------------------------
-// Row m of (D + diag I) times the broadcast vector v: four independent FMA
-// chains so the row's dot product is not one 112-long dependency chain.
+// Row m of (D + diag I) times the broadcast vector v, with row m of D read
+// from TMEM (lane m of accumulator tA) 32 columns at a time: the system stays
+// in TMEM for the whole solve instead of occupying NP registers. Four
+// independent FMA chains.
 template <int NP>
-__device__ __forceinline__ float matvec_row(const float (&arow)[NP], const float *v, float diag,
-                                            float vm) {
+__device__ __forceinline__ float matvec_tmem(uint32_t tA, const float *v, float diag, float vm) {
   float q0 = diag * vm, q1 = 0.f, q2 = 0.f, q3 = 0.f;
 #pragma unroll
-  for (int k = 0; k < NP; k += 4) {
-    const float4 p4 = *reinterpret_cast<const float4 *>(v + k);
-    q0 = fmaf(arow[k], p4.x, q0);
-    q1 = fmaf(arow[k + 1], p4.y, q1);
-    q2 = fmaf(arow[k + 2], p4.z, q2);
-    q3 = fmaf(arow[k + 3], p4.w, q3);
+  for (int c0 = 0; c0 < NP; c0 += 32) {
+    float d[32];
+    tc::tmem_ld32(tA + (uint32_t)c0, d);
+#pragma unroll
+    for (int k = 0; k < 32; k += 4) {
+      if (c0 + k < NP) {
+        const float4 p4 = *reinterpret_cast<const float4 *>(v + c0 + k);
+        q0 = fmaf(d[k], p4.x, q0);
+        q1 = fmaf(d[k + 1], p4.y, q1);
+        q2 = fmaf(d[k + 2], p4.z, q2);
+        q3 = fmaf(d[k + 3], p4.w, q3);
+      }
+    }
   }
   return (q0 + q1) + (q2 + q3);
 }
@@ -502,15 +518,17 @@ __device__ __noinline__ int ws_cholesky(float *S, float *dg, float *bv, float *x
   return refined ? 2 : 0;
 }
 
-// Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA; row n
-// sits in accumulator n mod 2 (with NG = 2 each group keeps one accumulator,
-// with NG = 1 the group alternates between both).
+// Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA. Row n
+// arrives in row slot n mod 2 (row_info / row_full / row_empty) and
+// accumulator n mod 4, which the group keeps until the row is solved: the
+// CG matrix-vector products read A_u from TMEM.
 template <int FP, int NP, typename LP, int NG>
 __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &sv,
                          const WsCtrl &c, unsigned char *mem, uint32_t tmem, int wg) {
   using L = WsLayout<FP, NP, NG>;
   constexpr int LDS = L::LDS, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
   static_assert(NTILES <= 128, "one warpgroup holds at most 128 Cholesky tiles");
+  static_assert(NP <= ws::kBufCols, "the system fits one accumulator");
   const int lt = threadIdx.x & 127, wl = (threadIdx.x >> 5) & 3;
   const Bar B{1 + wg, 128, lt};
   float *S = reinterpret_cast<float *>(mem);
@@ -523,52 +541,54 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   const bool live = m < f;
   ps[lt] = 0.f;  // L::kPs == 128 entries, one per thread
   B.sync();
-  unsigned parb = 0;  // phase parity per accumulator
+  unsigned rpar = 0, apar = 0;  // phase parities: row slots (2 bits), accumulators (4 bits)
   int rslot = 0;
   unsigned long long n_rows = 0, n_ref = 0, n_bad = 0, n_steps = 0, n_fb = 0, n_r0 = 0;
   const uint32_t tlane = tmem + ((uint32_t)(wl * 32) << 16);
-  for (int b = wg;; b = NG == 1 ? b ^ 1 : b) {
-    const unsigned par = (parb >> b) & 1u;
-    const uint32_t tbase = tlane + (uint32_t)b * ws::kBufCols;
-    bool ok = tc::mbar_wait_or_abort(&c.row_full[b], par, c.misc + 1);
+  const uint32_t bcol = (uint32_t)(a.ld_src & ~15);
+  const int bq = a.ld_src & 15;
+  for (long long n = wg;; n += NG) {
+    const int rb = (int)(n & 1), ab = (int)(n & (ws::kAcc - 1));
+    const uint32_t tA = tlane + (uint32_t)ab * ws::kBufCols;
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], (rpar >> rb) & 1u, c.misc + 1);
+    rpar ^= 1u << rb;
     if (!B.all(ok)) { ws_abort(a, c); break; }
-    const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[b]);
+    const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[rb]);
     const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
     B.sync();
-    if (lt == 0) tc::mbar_arrive(&c.row_empty[b]);
+    if (lt == 0) tc::mbar_arrive(&c.row_empty[rb]);
     if (info.x < 0) break;
     const int64_t u = info.x;
     const float reg = a.lambda * (float)info.y;
-    ok = tc::mbar_wait_or_abort(&c.acc_full[b], par, c.misc + 1);
-    parb ^= 1u << b;
+    // the warm start's load overlaps the wait for the accumulator
+    float x = (live && sv.x0 && info.z < 0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
+    ok = tc::mbar_wait_or_abort(&c.acc_full[ab], (apar >> ab) & 1u, c.misc + 1);
+    apar ^= 1u << ab;
     if (!B.all(ok)) { ws_abort(a, c); break; }
     tc::tc_fence_after();
-    // Thread m <- row m of D. Columns >= f and rows >= f of D are zero (zero
-    // padding of the gathered factors); column 128 holds b_u.
-    float arow[NP];
-#pragma unroll
-    for (int c0 = 0; c0 < NP; c0 += 16) {
-      float v[16];
-      tc::tmem_ld16(tbase + c0, v);
-#pragma unroll
-      for (int q = 0; q < 16; ++q) arow[c0 + q] = v[q];
-    }
-    float bm;
+    // b_u sits in column c_r = ld of D; rows >= f (no unknown) are ignored
+    float bm = 0.f;
     {
       float v[16];
-      tc::tmem_ld16(tbase + ws::kBCol, v);
-      bm = v[0];
+      tc::tmem_ld16(tA + bcol, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q == bq && live) bm = v[q];
     }
-    tc::tc_fence_before();
-    tc::mbar_arrive(&c.acc_empty[b]);  // the accumulator may be overwritten now
     if (info.z >= 0) {
       // A chunk of a split row: store the partial sums; the chunk that
-      // finishes last adds all of them, in chunk order, and solves the row.
+      // finishes last adds all of them, in chunk order, into its own
+      // accumulator and solves the row.
       float *P = plan.partial + ((size_t)info.z * 128 + m) * plan.part_ld;
 #pragma unroll
-      for (int cc = 0; cc < NP; cc += 4)
-        __stcg(reinterpret_cast<float4 *>(P + cc),
-               make_float4(arow[cc], arow[cc + 1], arow[cc + 2], arow[cc + 3]));
+      for (int c0 = 0; c0 < NP; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tA + (uint32_t)c0, v);
+#pragma unroll
+        for (int q = 0; q < 16; q += 4)
+          __stcg(reinterpret_cast<float4 *>(P + c0 + q),
+                 live ? make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]) : make_float4(0.f, 0.f, 0.f, 0.f));
+      }
       __stcg(P + NP, bm);
       __threadfence();
       B.sync();
@@ -579,25 +599,36 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       B.sync();
       const bool last = bad[1] != 0;
       B.sync();
-      if (!last) continue;
+      if (!last) {
+        tc::tc_fence_before();
+        tc::mbar_arrive(&c.acc_empty[ab]);
+        continue;
+      }
       __threadfence();
       const int base = plan.heavy_base[info.w], nch = plan.heavy_nchunks[info.w];
 #pragma unroll
-      for (int cc = 0; cc < NP; ++cc) arow[cc] = 0.f;
-      bm = 0.f;
-      for (int ch = 0; ch < nch; ++ch) {
-        const float *Q = plan.partial + ((size_t)(base + ch) * 128 + m) * plan.part_ld;
+      for (int c0 = 0; c0 < NP; c0 += 16) {
+        float v[16];
 #pragma unroll
-        for (int cc = 0; cc < NP; cc += 4) {
-          const float4 v = __ldcg(reinterpret_cast<const float4 *>(Q + cc));
-          arow[cc] += v.x;
-          arow[cc + 1] += v.y;
-          arow[cc + 2] += v.z;
-          arow[cc + 3] += v.w;
+        for (int q = 0; q < 16; ++q) v[q] = 0.f;
+        for (int ch = 0; ch < nch; ++ch) {
+          const float *Q = plan.partial + ((size_t)(base + ch) * 128 + m) * plan.part_ld + c0;
+#pragma unroll
+          for (int q = 0; q < 16; q += 4) {
+            const float4 w4 = __ldcg(reinterpret_cast<const float4 *>(Q + q));
+            v[q] += w4.x;
+            v[q + 1] += w4.y;
+            v[q + 2] += w4.z;
+            v[q + 3] += w4.w;
+          }
         }
-        bm += __ldcg(Q + NP);
+        tc::tmem_st16(tA + (uint32_t)c0, v);
       }
+      bm = 0.f;
+      for (int ch = 0; ch < nch; ++ch)
+        bm += __ldcg(plan.partial + ((size_t)(base + ch) * 128 + m) * plan.part_ld + NP);
       if (lt == 0) plan.heavy_count[info.w] = 0;  // ready for the next half-step
+      x = (live && sv.x0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
     }
     ++n_rows;
     uint32_t flags = 0;
@@ -607,14 +638,18 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       // Conjugate gradients on A_u = D + reg I, preconditioned by diag(A_u)
       // (Jacobi) unless disabled; three barriers per step.
       float dinv = live ? 1.f : 0.f;
-      if (sv.jacobi && live) {
+      if (sv.jacobi) {
         float dm = 0.f;
 #pragma unroll
-        for (int cc = 0; cc < NP; ++cc)
-          if (cc == m) dm = arow[cc];
-        dinv = 1.f / (dm + reg);
+        for (int c0 = 0; c0 < NP; c0 += 16) {
+          float v[16];
+          tc::tmem_ld16(tA + (uint32_t)c0, v);
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            if (c0 + q == m) dm = v[q];
+        }
+        if (live) dinv = 1.f / (dm + reg);
       }
-      float x = (live && sv.x0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
       if (!isfinite(x)) x = 0.f;
       float r = bm;
       if (sv.x0) {
@@ -623,7 +658,8 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
         // the start is never worse than zero in that norm.
         ps[m] = x;
         B.sync();
-        const float q0 = live ? matvec_row<NP>(arow, ps, reg, x) : 0.f;
+        float q0 = matvec_tmem<NP>(tA, ps, reg, x);
+        if (!live) q0 = 0.f;
         const float2 xs = group_sum2(x * bm, x * q0, red, rslot, B);
         float sc = xs.x / xs.y;
         if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
@@ -633,24 +669,25 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       if (!live) r = 0.f;
       float z = dinv * r;
       float p = z;
-      float2 t = group_sum2(r * z, r * r, red, rslot, B);
-      float gamma = t.x;
-      const float bb = group_sum2(bm * bm, 0.f, red, rslot, B).x;
+      const float4 t0 = group_sum4(make_float4(r * z, r * r, bm * bm, 0.f), red, rslot, B);
+      float gamma = t0.x;
+      const float bb = t0.z;
       const float target = sv.cg_tol2 * bb;
-      if (lt == 0 && bb > 0.f) n_r0 += (unsigned long long)(1e6f * sqrtf(t.y / bb));
-      bool conv = t.y <= target;
+      if (lt == 0 && bb > 0.f) n_r0 += (unsigned long long)(1e6f * sqrtf(t0.y / bb));
+      bool conv = t0.y <= target;
       int it = 0;
       while (!conv && it < sv.cg_max_steps) {
         ps[m] = p;
         B.sync();
-        const float w = matvec_row<NP>(arow, ps, reg, p);
+        float w = matvec_tmem<NP>(tA, ps, reg, p);
+        if (!live) w = 0.f;
         const float pq = group_sum2(p * w, 0.f, red, rslot, B).x;
         if (!(pq > 0.f)) break;  // not positive definite along p: fall back
         const float alpha = gamma / pq;
         x = fmaf(alpha, p, x);
         r = fmaf(-alpha, w, r);
         z = dinv * r;
-        t = group_sum2(r * z, r * r, red, rslot, B);
+        const float2 t = group_sum2(r * z, r * r, red, rslot, B);
         ++it;
         conv = t.y <= target;
         p = fmaf(t.x / gamma, p, z);
@@ -667,12 +704,21 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       B.sync();
     }
     if (!solved) {
-      if (m < FP) {
+      // the system into shared memory for the register-tile Cholesky
 #pragma unroll
-        for (int cc = 0; cc < FP; ++cc) {
-          const float v = cc < NP ? arow[cc] : 0.f;
-          S[m * LDS + cc] = (m < f && cc < f) ? v : (m == cc ? 1.f : 0.f);
+      for (int c0 = 0; c0 < NP; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tA + (uint32_t)c0, v);
+        if (m < FP) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int cc = c0 + q;
+            if (cc < FP) S[m * LDS + cc] = (m < f && cc < f) ? v[q] : (m == cc ? 1.f : 0.f);
+          }
         }
+      }
+      if (m < FP) {
+        for (int cc = NP; cc < FP; ++cc) S[m * LDS + cc] = m == cc ? 1.f : 0.f;
         bv[m] = bm;
       }
       B.sync();
@@ -687,6 +733,8 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       if (live) xm = xv[m];
       B.sync();
     }
+    tc::tc_fence_before();
+    tc::mbar_arrive(&c.acc_empty[ab]);  // the accumulator may be overwritten now
     if (live) {
       a.dst[u * a.ld_dst + m] = xm;
       if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[u * a.ld_dst_lp + m] = LP(xm);
@@ -714,8 +762,8 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
   c.full = reinterpret_cast<uint64_t *>(ctrl);
   c.empty = c.full + ws::NS;
   c.acc_full = c.empty + ws::NS;
-  c.acc_empty = c.acc_full + 2;
-  c.row_full = c.acc_empty + 2;
+  c.acc_empty = c.acc_full + ws::kAcc;
+  c.row_full = c.acc_empty + ws::kAcc;
   c.row_empty = c.row_full + 2;
   c.drain = c.row_empty + 2;
   c.stage_info = reinterpret_cast<int4 *>(ctrl + L::kBars);
@@ -728,9 +776,11 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
       tc::mbar_init(&c.full[i], ws::kFullCount);
       tc::mbar_init(&c.empty[i], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < ws::kAcc; ++b) {
       tc::mbar_init(&c.acc_full[b], 1);
       tc::mbar_init(&c.acc_empty[b], 128);
+    }
+    for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&c.row_full[b], 1);
       tc::mbar_init(&c.row_empty[b], 1);
     }
@@ -781,7 +831,7 @@ static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
   using L = WsLayout<FP, NP, NG>;
   WsGeom g;
   g.nj = a.ld_src / 8;
-  if (a.ld_src % 8 != 0 || a.ld_src > 128 || NP < a.f || FP < a.f || plan.part_ld < NP + 1)
+  if (a.ld_src % 8 != 0 || a.ld_src > 120 || NP < a.f || FP < a.f || plan.part_ld < NP + 1)
     return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
   auto kern = rows_tc_ws_kernel<FP, NP, LP, NG>;
@@ -789,7 +839,8 @@ static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
   if (err != cudaSuccess) return err;
   int64_t grid = num_sms;
   if (grid > plan.nitems) grid = plan.nitems > 0 ? plan.nitems : 1;
-  const uint32_t idesc = tc::make_idesc(lp_kind == kLpBf16 ? 1 : 0, ws::kN);
+  const int nmma = ((std::max(NP, a.ld_src + 1) + 15) / 16) * 16;  // B columns incl. c_r
+  const uint32_t idesc = tc::make_idesc(lp_kind == kLpBf16 ? 1 : 0, nmma);
   kern<<<(unsigned)grid, ws::threads<NG>(), L::kTotal, st>>>(a, idesc, sv, g, plan);
   return cudaGetLastError();
 }
