@@ -96,7 +96,7 @@ typedef struct als_options {
   int32_t cg_jacobi;       /* 1: diagonal (Jacobi) preconditioner for CG (default 0:
                               it slowed convergence on the benchmark matrices) */
   int32_t solver_groups;   /* solver warpgroups per SM in the tensor-core kernel:
-                              0 = chosen by the engine, 1 or 2                   */
+                              0 = chosen by the engine, 1, 2 or 3               */
   int32_t reserved[3];
 } als_options;
 
@@ -111,7 +111,8 @@ typedef struct als_stats {
   uint64_t cg_r0_micro;     /* sum over CG rows of the starting relative residual
                                |b - A x0| / |b| (x0 after optimal scaling), x 1e6:
                                a measure of the warm start's quality          */
-  uint64_t reserved[1];
+  uint32_t solver_groups[2]; /* warpgroup count the autotuner chose for the users /
+                                items side (0: not tuned, or fixed by the options) */
 } als_stats;
 
 void als_default_options(als_options *opt);
@@ -178,9 +179,15 @@ int als_half_step(int64_t m, int64_t n, int32_t f, const int64_t *d_row_ptr,
                   float *d_dst, int32_t ld_dst, float lambda, const als_options *opt,
                   void *d_work, size_t work_bytes, cudaStream_t stream);
 
-/* The same FP32 half-step without a workspace argument: its scratch (visiting
- * order, row queue, counters) is a file-scope __device__ array sized for at
- * most ALS_STATIC_MAX_ROWS rows (about 4 MiB), so a call allocates nothing.
+/* The same FP32 half-step without a workspace argument, for callers that
+ * cannot call cudaMalloc: a process whose device memory is already handed to
+ * another allocator's pool (a Spark executor or PyTorch process whose pooling
+ * allocator reserves the GPU, so a raw cudaMalloc fails or fragments it), or
+ * a caller that must not pay the device-wide synchronisation that
+ * cudaMalloc/cudaFree can cause. Its scratch (visiting order, row queue,
+ * counters) is a file-scope __device__ array sized for at most
+ * ALS_STATIC_MAX_ROWS rows (about 4 MiB, held on every GPU that loads the
+ * library until the process exits), so a call allocates nothing.
  * Larger m is rejected with ALS_ERR_INVALID. The first call on each device
  * looks the array up with cudaGetSymbolAddress; make that first call before
  * any stream capture. Calls that overlap in time (two streams, two host

@@ -1,6 +1,10 @@
 """The allocation-free FP32 half-step (als_half_step_static, scratch in a
 file-scope device array) against the workspace entry point als_half_step on the
-same seeded inputs, on two calls in a row, plus its size limit.
+same seeded inputs, on two calls in a row, plus its size limit. The entry point
+exists for callers that cannot call cudaMalloc (their GPU memory belongs to a
+pooling allocator, or they must avoid the synchronisation an allocation can
+cause); the second call checks that the shared array's leftover contents from
+the first call do not leak into the result.
 
 Tolerance: the FP32 form's, per-row relative L2 difference <= 1e-3 (both
 entries run the same kernel, so the results normally agree exactly)."""
