@@ -298,16 +298,29 @@ def run_engine(args):
     if args.warm == "mlp":
         launches_per_step += 2 + 3 * (-(-r.m // 32768) + -(-r.n // 32768))
 
-    # roofline of the dominant kernel: the fused rows kernel, one launch per half-step
+    # roofline of the dominant kernel: the fused rows kernel, one launch per half-step.
+    # Bound: the gather of the rated factor rows (bytes per rating: column index,
+    # rating, one factor row of f elements at s bytes; per row: pointer, warm
+    # start read, FP32 + copy write), over the measured HBM copy bandwidth; the
+    # SYRK flops over the tensor peak are reported beside it.
     hbm, tf_burst, tf_sust, src = peaks()
-    per_side = lambda nnz, rows: nnz * f * (f + 1) + 2 * nnz * f + rows * (f ** 3 / 3 + 2 * f * f)
+    s_el = 4 if args.precision == "fp32" else 2
+    side_bytes = lambda nnz, rows: nnz * (8 + f * s_el) + rows * (8 + 4 * f + 4 * f + s_el * f)
     avg_launch_s = float(np.concatenate([users_ms, items_ms]).mean()) / 1e3
-    avg_flops = (per_side(r.nnz, r.m) + per_side(r.nnz, r.n)) / 2
-    achieved = avg_flops / avg_launch_s / 1e12
-    roof = {"bound": "tensor", "achieved": round(achieved, 3), "peak": tf_sust, "unit": "TFLOP/s",
-            "frac": round(achieved / tf_sust, 4), "traffic": None,
-            "peak_kind": f"{src} bf16 dense sustained",
-            "kernel": "rows kernel (gather + hermitian + solve), both sides",
+    avg_bytes = (side_bytes(r.nnz, r.m) + side_bytes(r.nnz, r.n)) / 2
+    achieved_gbs = avg_bytes / avg_launch_s / 1e9
+    syrk_tflops = r.nnz * f * (f + 1) / avg_launch_s / 1e12
+    items_gbs = side_bytes(r.nnz, r.n) / (float(items_ms.mean()) / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved_gbs / hbm, 4), "traffic": None,
+            "peak_kind": f"{src} HBM copy bandwidth",
+            "kernel": "rows kernel (gather + hermitian + solve), mean of the two launches per step",
+            "bytes_per_launch": round(avg_bytes), "bytes_formula": "nnz*(8+f*s) + rows*(8+8f+f*s)",
+            "items_launch": {"ms": round(float(items_ms.mean()), 3), "achieved": round(items_gbs, 1),
+                             "frac": round(items_gbs / hbm, 4)},
+            "tensor": {"syrk_flops_per_launch": r.nnz * f * (f + 1), "achieved_tflops": round(syrk_tflops, 2),
+                       "peak": tf_sust, "frac": round(syrk_tflops / tf_sust, 4),
+                       "peak_kind": f"{src} bf16 dense sustained"},
             "users_ms": round(float(users_ms.mean()), 3), "items_ms": round(float(items_ms.mean()), 3)}
 
     line = None

@@ -64,10 +64,14 @@ class Options(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("rows_solved", c_u64), ("rows_refined", c_u64), ("rows_not_spd", c_u64),
                 ("cg_steps", c_u64), ("cg_fallbacks", c_u64), ("kernel_errors", c_u64),
-                ("cg_r0_micro", c_u64), ("reserved", c_u64 * 1)]
+                ("cg_r0_micro", c_u64), ("solver_groups", ctypes.c_uint32 * 2)]
 
     def as_dict(self) -> dict:
-        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
+        out = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            out[k] = list(v) if k == "solver_groups" else int(v)
+        return out
 
 
 class SynthSpec(ctypes.Structure):

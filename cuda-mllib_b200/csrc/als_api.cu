@@ -56,7 +56,7 @@ int check_options(const als_options &o, int f) {
     return fail(ALS_ERR_UNSUPPORTED, "tensor-core form supports rank f in 16..128");
   }
   if (o.cg_max_steps < 0 || o.cg_max_steps > 256) return fail(ALS_ERR_INVALID, "cg_max_steps");
-  if (o.solver_groups < 0 || o.solver_groups > 2) return fail(ALS_ERR_INVALID, "solver_groups must be 0, 1 or 2");
+  if (o.solver_groups < 0 || o.solver_groups > 3) return fail(ALS_ERR_INVALID, "solver_groups must be 0 .. 3");
   if (o.warm_start < ALS_WARM_ZERO || o.warm_start > ALS_WARM_MLP)
     return fail(ALS_ERR_INVALID, "unknown warm start");
   if (o.warm_start == ALS_WARM_MLP &&
@@ -142,7 +142,19 @@ struct als_model {
   int ldf = 0;
   int halfsteps[2] = {0, 0};
   void *mlp_block = nullptr;
+  // solver-warpgroup autotuning per side (options.solver_groups == 0)
+  int tuned[2] = {0, 0};     // chosen warpgroup count, 0 while tuning
+  int tune_idx[2] = {0, 0};  // half-steps timed so far
+  float tune_ms[2][3] = {};
+  cudaEvent_t tev[2] = {nullptr, nullptr};
 };
+
+namespace {
+// Warpgroup counts tried for a side, in this order: the first and last runs
+// bracket the middle one, so the steady drop of CG steps from one iteration
+// to the next cancels out of the comparison.
+constexpr int kTuneSeq[3] = {2, 3, 2};
+}  // namespace
 
 extern "C" {
 
@@ -203,6 +215,8 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
   als_model *M = new als_model();
   M->m = m; M->n = n; M->f = f; M->nnz = nnz; M->opt = o;
   M->num_sms = device_sm_count();
+  for (int i = 0; i < 2; ++i)
+    if (cudaEventCreate(&M->tev[i]) != cudaSuccess) M->tev[i] = nullptr;  // no events: no tuning
   const int kind = lp_kind_of(o.precision);
   M->lp_ld = kind == kLpNone ? 0 : tc_padded_ld(f);
   // one allocation: factors, low-precision copies, orders, queues, flags, counters
@@ -281,6 +295,8 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
 void als_model_destroy(als_model *M) {
   if (!M) return;
   if (M->graph) cudaGraphExecDestroy(M->graph);
+  for (int i = 0; i < 2; ++i)
+    if (M->tev[i]) cudaEventDestroy(M->tev[i]);
   for (int s = 0; s < 2; ++s) {
     mlp_destroy(M->net[s]);
     cudaFree(M->side[s].plan_mem);
@@ -323,9 +339,15 @@ static cudaError_t model_half(als_model *M, int side, float lambda, cudaStream_t
   const float *x0 = (M->opt.warm_start == ALS_WARM_PREVIOUS) ? dst32 : nullptr;
   bool train = false;
   if (M->opt.warm_start == ALS_WARM_MLP) {
-    // features of this side's rows against the fixed factor (BF16/FP16 copy)
-    cudaError_t e = mlp_features(S.rows, M->f, S.ptr, S.idx, S.val, src_lp, M->lp_ld,
-                                 lp_kind_of(M->opt.precision), M->feat[side], M->ldf, st);
+    // features of this side's rows against the fixed factor (BF16/FP16 copy),
+    // over the side's work plan when it has one
+    cudaError_t e = cudaErrorNotSupported;
+    if (S.has_plan)
+      e = mlp_features_plan(S.plan, M->f, S.idx, S.val, src_lp, M->lp_ld,
+                            lp_kind_of(M->opt.precision), M->feat[side], M->ldf, st);
+    if (e == cudaErrorNotSupported)
+      e = mlp_features(S.rows, M->f, S.ptr, S.idx, S.val, src_lp, M->lp_ld,
+                       lp_kind_of(M->opt.precision), M->feat[side], M->ldf, st);
     if (e != cudaSuccess) return e;
     train = M->halfsteps[side] < M->opt.mlp_train_iters;
     if (train) {
@@ -336,9 +358,39 @@ static cudaError_t model_half(als_model *M, int side, float lambda, cudaStream_t
       x0 = M->x0[side];
     }
   }
-  cudaError_t e = run_rows(S, M->f, lambda, M->opt, src32, M->f, src_lp, M->lp_ld, dst32, dst_lp,
-                           M->ctr, x0, M->num_sms, st);
+  // Autotuner: with solver_groups = 0 each side's first half-steps time the
+  // candidate warpgroup counts of the tensor-core kernel (not while a graph is
+  // being captured); the faster one is kept for the side.
+  als_options o = M->opt;
+  bool timing = false;
+  if (o.solver_groups == 0 && S.has_plan && lp_kind_of(o.precision) != kLpNone) {
+    if (M->tuned[side]) {
+      o.solver_groups = M->tuned[side];
+    } else {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      cudaStreamIsCapturing(st, &cs);
+      if (cs == cudaStreamCaptureStatusNone && M->tev[0] && M->tev[1]) {
+        o.solver_groups = kTuneSeq[M->tune_idx[side]];
+        timing = true;
+      }
+    }
+  }
+  cudaError_t e;
+  if (timing && (e = cudaEventRecord(M->tev[0], st)) != cudaSuccess) return e;
+  e = run_rows(S, M->f, lambda, o, src32, M->f, src_lp, M->lp_ld, dst32, dst_lp, M->ctr, x0,
+               M->num_sms, st);
   if (e != cudaSuccess) return e;
+  if (timing) {
+    float ms = 0.f;
+    if ((e = cudaEventRecord(M->tev[1], st)) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(M->tev[1])) != cudaSuccess) return e;
+    if ((e = cudaEventElapsedTime(&ms, M->tev[0], M->tev[1])) != cudaSuccess) return e;
+    M->tune_ms[side][M->tune_idx[side]++] = ms;
+    if (M->tune_idx[side] == 3) {
+      const float t2 = 0.5f * (M->tune_ms[side][0] + M->tune_ms[side][2]), t3 = M->tune_ms[side][1];
+      M->tuned[side] = t3 < t2 ? 3 : 2;
+    }
+  }
   if (M->opt.warm_start == ALS_WARM_MLP) {
     if (train)
       e = mlp_train(M->net[side], S.rows, M->opt.mlp_batch, M->opt.mlp_steps, M->feat[side],
@@ -439,6 +491,8 @@ int als_model_stats(als_model *M, als_stats *out, int32_t reset) {
   out->cg_fallbacks = c.cg_fallback;
   out->kernel_errors = (uint64_t)(c.error != 0);
   out->cg_r0_micro = c.r0_micro;
+  out->solver_groups[0] = (uint32_t)M->tuned[0];
+  out->solver_groups[1] = (uint32_t)M->tuned[1];
   if (reset) ALS_TRY(cudaMemset(M->ctr, 0, sizeof(Counters)), "stats reset");
   return ALS_OK;
 }
@@ -508,7 +562,21 @@ int als_features(int64_t m, int32_t f, const int64_t *ptr, const int32_t *col, c
                  cudaStream_t st) {
   if (m < 0 || f <= 0 || f > 128 || !ptr || !src || !F || ld_src < f || ldf < 2 * f + 1)
     return fail(ALS_ERR_INVALID, "bad args");
-  ALS_TRY(mlp_features(m, f, ptr, col, val, src, ld_src, lp_kind_of(prec), F, ldf, st), "als_features");
+  const int kind = lp_kind_of(prec);
+  if (m > 0 && kind != kLpNone && ld_src % 8 == 0) {
+    // the model's path: a work plan over the rows (long rows split), then the plan kernel
+    WsPlan plan;
+    void *mem = nullptr;
+    cudaError_t e = plan_ws(ptr, 0, m, device_sm_count(), 128, 0, &plan, &mem, st);
+    if (e == cudaSuccess) e = mlp_features_plan(plan, f, col, val, src, ld_src, kind, F, ldf, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(mem);
+    if (e != cudaErrorNotSupported) {
+      ALS_TRY(e, "als_features");
+      return ALS_OK;
+    }
+  }
+  ALS_TRY(mlp_features(m, f, ptr, col, val, src, ld_src, kind, F, ldf, st), "als_features");
   return ALS_OK;
 }
 
@@ -733,7 +801,10 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
 // ---------------------------------------------------------------------------
 // als_half_step_static: the stand-alone FP32 half-step with its scratch (the
 // degree-binned visiting order, the row-queue head and the counters) in a
-// file-scope device array, so that a call allocates nothing.
+// file-scope device array, so that a call allocates nothing. It serves callers
+// that cannot call cudaMalloc: their device memory belongs to another
+// allocator's pool, or they must not take the synchronisation that
+// cudaMalloc/cudaFree can cause.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr size_t kStaticQueueOff = (sizeof(int32_t) * (size_t)ALS_STATIC_MAX_ROWS + 255) / 256 * 256;

@@ -44,6 +44,9 @@ struct alignas(16) WorkItem {
   int heavy;       // index of the split row; -1 otherwise
 };
 
+// Floats of one fallback Cholesky tile in global scratch (f <= 112: 112 x 113).
+constexpr int kCholFloats = 112 * 113;
+
 struct WsPlan {
   const WorkItem *items = nullptr;
   int nitems = 0;
@@ -52,7 +55,9 @@ struct WsPlan {
   unsigned *heavy_count = nullptr;     // per split row: chunks finished (reset by the last)
   float *partial = nullptr;            // [slots][128][part_ld]
   int part_ld = 0;
-  int src_rows = 0;                    // rows of the source factor matrix (TMA bounds)
+  int src_rows = 0;                    // rows of the source factor matrix (gather bounds)
+  float *chol = nullptr;               // [ctas][3][kCholFloats] fallback Cholesky tiles
+  int ctas = 0;                        // CTAs the scratch covers: a launch uses at most this many
 };
 
 // Host-side planning of a side's rows [begin, begin + count): items sorted by
@@ -102,6 +107,11 @@ int64_t mlp_param_count(int f);
 cudaError_t mlp_features(int64_t m, int f, const int64_t *row_ptr, const int32_t *col,
                          const float *val, const void *src, int ld_src, int lp_kind, void *F,
                          int ldf, cudaStream_t st);
+// The same features over a side's work plan (16-bit factors only): long rows
+// are split across blocks like the half-step kernel splits them.
+cudaError_t mlp_features_plan(const WsPlan &plan, int f, const int32_t *col, const float *val,
+                              const void *src, int ld_src, int lp_kind, void *F, int ldf,
+                              cudaStream_t st);
 cudaError_t mlp_infer(void *net, int64_t m, const void *F, float *X0, int ldx, cudaStream_t st);
 cudaError_t mlp_train(void *net, int64_t m, int64_t batch, int steps, const void *F,
                       const float *T, int ldt, float lr, uint64_t seed, cudaStream_t st);

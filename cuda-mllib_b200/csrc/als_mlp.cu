@@ -262,6 +262,166 @@ __global__ void __launch_bounds__(256) features_kernel(int64_t m, int f, const i
   }
 }
 
+// The same features from a 16-bit factor copy (row stride ld a multiple of 8):
+// each half-warp takes one rating, its lanes one 16-byte piece (8 elements)
+// of the rated factor row each; a warp takes 32 ratings per round, their
+// column indices and ratings read in one coalesced load and handed out by
+// shuffles, so sixteen factor-row loads can be in flight per warp.
+template <typename LP>
+__global__ void __launch_bounds__(256) features_lp_kernel(int64_t m, int f, const int64_t *row_ptr,
+                                                          const int32_t *col, const float *val,
+                                                          const LP *src, int ld_src,
+                                                          __nv_bfloat16 *F, int ldf) {
+  __shared__ float part[8][2][128];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, h = lane >> 4, j = lane & 15;
+  const int nj = ld_src / 8;
+  for (int64_t u = blockIdx.x; u < m; u += gridDim.x) {
+    const int64_t S0 = row_ptr[u], E0 = row_ptr[u + 1];
+    float b[8], d[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) b[q] = d[q] = 0.f;
+    for (int64_t q0 = S0 + 32 * w; q0 < E0; q0 += 256) {
+      const int64_t q = q0 + lane;
+      const int cl = q < E0 ? col[q] : -1;
+      const float rl = q < E0 ? val[q] : 0.f;
+#pragma unroll 8
+      for (int k = 0; k < 32; k += 2) {
+        const int ci = __shfl_sync(0xffffffffu, cl, k + h);
+        const float ri = __shfl_sync(0xffffffffu, rl, k + h);
+        if (ci >= 0 && j < nj) {
+          const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(src + (size_t)ci * ld_src) + j);
+          const LP *v = reinterpret_cast<const LP *>(&raw);
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            const float x = (float)v[t];
+            b[t] = fmaf(ri, x, b[t]);
+            d[t] = fmaf(x, x, d[t]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      b[t] += __shfl_xor_sync(0xffffffffu, b[t], 16);
+      d[t] += __shfl_xor_sync(0xffffffffu, d[t], 16);
+    }
+    if (h == 0) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        part[w][0][8 * j + t] = b[t];
+        part[w][1][8 * j + t] = d[t];
+      }
+    }
+    __syncthreads();
+    const float n = (float)(E0 - S0), inv = n > 0.f ? 1.f / n : 0.f;
+    __nv_bfloat16 *o = F + u * ldf;
+    for (int i = threadIdx.x; i < ldf; i += blockDim.x) {
+      float v = 0.f;
+      if (i < 2 * f) {
+        const int hh = i < f ? 0 : 1, c = i < f ? i : i - f;
+        for (int k = 0; k < 8; ++k) v += part[k][hh][c];
+        v *= inv;
+      } else if (i == 2 * f) {
+        v = log1pf(n) * 0.125f;
+      }
+      o[i] = __float2bfloat16(v);
+    }
+    __syncthreads();
+  }
+}
+
+// Features driven by a side's work plan: one block per work item (a row, or
+// a chunk of a row too long for one block), largest first. A chunk stores its
+// sums in its partial slot; the chunk that finishes last adds the row's slots
+// in chunk order (deterministic) and writes the features.
+template <typename LP>
+__global__ void __launch_bounds__(256) features_plan_kernel(WsPlan plan, int f, const int32_t *col,
+                                                            const float *val, const LP *src,
+                                                            int ld_src, __nv_bfloat16 *F, int ldf) {
+  __shared__ float part[8][2][128];
+  __shared__ float tot[256];
+  __shared__ int last;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, h = lane >> 4, j = lane & 15;
+  const int nj = ld_src / 8;
+  for (int64_t idx = blockIdx.x; idx < plan.nitems; idx += gridDim.x) {
+    const WorkItem it = plan.items[idx];
+    const int64_t S0 = it.s, E0 = it.e;
+    float b[8], d[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) b[q] = d[q] = 0.f;
+    for (int64_t q0 = S0 + 32 * w; q0 < E0; q0 += 256) {
+      const int64_t q = q0 + lane;
+      const int cl = q < E0 ? col[q] : -1;
+      const float rl = q < E0 ? val[q] : 0.f;
+#pragma unroll 8
+      for (int k = 0; k < 32; k += 2) {
+        const int ci = __shfl_sync(0xffffffffu, cl, k + h);
+        const float ri = __shfl_sync(0xffffffffu, rl, k + h);
+        if (ci >= 0 && j < nj) {
+          const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(src + (size_t)ci * ld_src) + j);
+          const LP *v = reinterpret_cast<const LP *>(&raw);
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            const float x = (float)v[t];
+            b[t] = fmaf(ri, x, b[t]);
+            d[t] = fmaf(x, x, d[t]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      b[t] += __shfl_xor_sync(0xffffffffu, b[t], 16);
+      d[t] += __shfl_xor_sync(0xffffffffu, d[t], 16);
+    }
+    if (h == 0) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        part[w][0][8 * j + t] = b[t];
+        part[w][1][8 * j + t] = d[t];
+      }
+    }
+    __syncthreads();
+    {
+      const int i = threadIdx.x, hh = i >> 7, c = i & 127;
+      float v = 0.f;
+      for (int k = 0; k < 8; ++k) v += part[k][hh][c];
+      tot[i] = v;
+    }
+    __syncthreads();
+    if (it.part >= 0) {
+      float *P = plan.partial + (size_t)it.part * 128 * plan.part_ld;
+      __stcg(P + threadIdx.x, tot[threadIdx.x]);
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const unsigned done = atomicAdd(&plan.heavy_count[it.heavy], 1u) + 1;
+        last = done == (unsigned)plan.heavy_nchunks[it.heavy] ? 1 : 0;
+      }
+      __syncthreads();
+      if (!last) continue;
+      __threadfence();
+      const int base = plan.heavy_base[it.heavy], nch = plan.heavy_nchunks[it.heavy];
+      float v = 0.f;
+      for (int ch = 0; ch < nch; ++ch)
+        v += __ldcg(plan.partial + (size_t)(base + ch) * 128 * plan.part_ld + threadIdx.x);
+      __syncthreads();
+      tot[threadIdx.x] = v;
+      if (threadIdx.x == 0) plan.heavy_count[it.heavy] = 0;  // ready for the next use
+      __syncthreads();
+    }
+    const float n = (float)it.deg, inv = n > 0.f ? 1.f / n : 0.f;
+    __nv_bfloat16 *o = F + (size_t)it.u * ldf;
+    for (int i = threadIdx.x; i < ldf; i += blockDim.x) {
+      float v = 0.f;
+      if (i < 2 * f) v = (i < f ? tot[i] : tot[128 + i - f]) * inv;
+      else if (i == 2 * f) v = log1pf(n) * 0.125f;
+      o[i] = __float2bfloat16(v);
+    }
+    __syncthreads();
+  }
+}
+
 // dY = 2 (Y - T) / (B f) for the loss mean_b |Y_b - T_b|^2 / f; loss partials in FP64.
 __global__ void loss_grad_kernel(int64_t B, int f, const float *Y, int ldy, const float *T,
                                  int ldt, __nv_bfloat16 *dY, float *dY32, int lddy,
@@ -591,13 +751,39 @@ int mlp_ldf(const void *p) { return ((const mlp::Net *)p)->ldf; }
 int64_t mlp_nparam(const void *p) { return ((const mlp::Net *)p)->nparam; }
 int *mlp_error(const void *p) { return ((const mlp::Net *)p)->error; }
 
+cudaError_t mlp_features_plan(const WsPlan &plan, int f, const int32_t *col, const float *val,
+                              const void *src, int ld_src, int lp_kind, void *F, int ldf,
+                              cudaStream_t st) {
+  if (plan.nitems <= 0) return cudaSuccess;
+  if (f > 128 || ld_src % 8 != 0 || ld_src > 128 || (reinterpret_cast<uintptr_t>(src) & 15) != 0 ||
+      plan.part_ld * 128 < 256 || (lp_kind != kLpBf16 && lp_kind != kLpFp16))
+    return cudaErrorNotSupported;
+  const unsigned grid = (unsigned)std::min<int64_t>(plan.nitems, (int64_t)device_sm_count() * 8);
+  if (lp_kind == kLpBf16)
+    mlp::features_plan_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
+        plan, f, col, val, (const __nv_bfloat16 *)src, ld_src, (__nv_bfloat16 *)F, ldf);
+  else
+    mlp::features_plan_kernel<__half><<<grid, 256, 0, st>>>(
+        plan, f, col, val, (const __half *)src, ld_src, (__nv_bfloat16 *)F, ldf);
+  return cudaGetLastError();
+}
+
 cudaError_t mlp_features(int64_t m, int f, const int64_t *row_ptr, const int32_t *col,
                          const float *val, const void *src, int ld_src, int lp_kind, void *F,
                          int ldf, cudaStream_t st) {
   if (m <= 0) return cudaSuccess;
   if (f > 128) return cudaErrorInvalidValue;
   const unsigned grid = (unsigned)std::min<int64_t>(m, 148 * 8);
-  if (lp_kind == kLpBf16)
+  const bool pieces = ld_src % 8 == 0 && ld_src <= 128 &&
+                      (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+  if (lp_kind == kLpBf16 && pieces)
+    mlp::features_lp_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
+        m, f, row_ptr, col, val, (const __nv_bfloat16 *)src, ld_src, (__nv_bfloat16 *)F, ldf);
+  else if (lp_kind == kLpFp16 && pieces)
+    mlp::features_lp_kernel<__half><<<grid, 256, 0, st>>>(m, f, row_ptr, col, val,
+                                                          (const __half *)src, ld_src,
+                                                          (__nv_bfloat16 *)F, ldf);
+  else if (lp_kind == kLpBf16)
     mlp::features_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
         m, f, row_ptr, col, val, (const __nv_bfloat16 *)src, ld_src, (__nv_bfloat16 *)F, ldf);
   else if (lp_kind == kLpFp16)

@@ -47,8 +47,8 @@ namespace als {
 
 namespace ws {
 // NG solver warpgroups (warps 0 .. 4 NG - 1), then the producer and MMA warps.
-// With NG = 2 an SM sub-partition holds three warps, which caps a thread at
-// 168 registers; NG = 1 leaves two per sub-partition (up to 255).
+// Registers per thread are capped by the busiest SM sub-partition: 255 with
+// NG = 1 (two warps), 168 with NG = 2 (three), 128 with NG = 3 (four).
 template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG + 64; }
 template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }
 template <int NG> __host__ __device__ constexpr int mma_warp() { return 4 * NG + 1; }
@@ -57,6 +57,7 @@ constexpr int KS = 64;                            // ratings per stage
 constexpr int kAtom = (KS / 8) * 1024;            // one 64-element MN atom of a stage
 constexpr int kStageBytes = 2 * kAtom;            // tile columns 0-63 and 64-127
 constexpr int kAcc = 4;                           // TMEM accumulators (row n -> n mod 4)
+constexpr int kMaxGroups = 3;                     // solver warpgroups per CTA at most
 constexpr int kBufCols = 128;                     // TMEM columns per accumulator
 constexpr int kTmemCols = kAcc * kBufCols;        // all 512 columns
 constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
@@ -68,11 +69,13 @@ struct WsGeom {
   int nj;  // 16-byte pieces per factor row (ld_src / 8, at most 16)
 };
 
+// Per solver warpgroup: vectors of the fallback Cholesky (its f x f tile lives
+// in global scratch, plan.chol), the CG broadcast vector and reduction slots.
 template <int FP, int NP, int NG>
 struct WsLayout {
   static constexpr int LDS = FP + 1;
-  static constexpr size_t kS = (size_t)FP * LDS * 4;
-  static constexpr size_t oDg = kS, oBv = oDg + FP * 4, oXv = oBv + FP * 4, oTmp = oXv + FP * 4;
+  static_assert((size_t)FP * LDS <= (size_t)kCholFloats, "Cholesky tile fits its scratch");
+  static constexpr size_t oDg = 0, oBv = oDg + FP * 4, oXv = oBv + FP * 4, oTmp = oXv + FP * 4;
   static constexpr size_t oPs = (oTmp + FP * 4 + 15) / 16 * 16;
   static constexpr int kPs = 128;  // CG broadcast vector: one entry per thread of the warpgroup
   static_assert(NP <= kPs, "the broadcast vector covers every accumulator column");
@@ -82,10 +85,11 @@ struct WsLayout {
   static constexpr size_t kSolver = (oMisc + 16 + 127) / 128 * 128;
   static constexpr size_t oSolver = (size_t)ws::NS * ws::kStageBytes;
   static constexpr size_t oCtrl = oSolver + NG * kSolver;
-  // full, empty per stage; acc_full, acc_empty per accumulator; row_full,
-  // row_empty per row slot; drain; one spare (16-byte multiple)
-  static constexpr size_t kBars = 8 * (2 * ws::NS + 2 * ws::kAcc + 6);
-  static constexpr size_t kCtrl = kBars + 16 * (ws::NS + 2) + 16;
+  // full, empty per stage; acc_full, acc_empty, row_full, row_empty per
+  // accumulator (row n uses accumulator and row slot n mod kAcc); drain; one
+  // spare (16-byte multiple)
+  static constexpr size_t kBars = 8 * (2 * ws::NS + 4 * ws::kAcc + 2);
+  static constexpr size_t kCtrl = kBars + 16 * (ws::NS + ws::kAcc) + 16;
   static constexpr size_t oRing = oCtrl + kCtrl;  // 16-byte aligned
   static constexpr size_t kTotal = 1024 + oRing + (size_t)ws::DI * ws::kRingSlot;
   static_assert(kCtrl % 16 == 0 && ws::kRingSlot % 16 == 0, "ring alignment");
@@ -281,7 +285,7 @@ __device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &pl
   }
 }
 
-template <typename LP>
+template <typename LP, int NG>
 __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &g,
                            const WsCtrl &c, unsigned char *stages, unsigned char *ring,
                            unsigned long long &n_empty_rows) {
@@ -302,10 +306,9 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     if (__any_sync(0xffffffffu, h1.w == 0 || c.misc[1] != 0)) break;  // warp-uniform exit
     const int kc = h1.x, first = h1.y, last = h1.z;
     if (first) {
-      // row nrow: row slot nrow mod 2 for the solver handshake, accumulator
-      // nrow mod kAcc for the MMA
-      const int b = (int)(nrow & 1);
+      // row nrow: row slot and accumulator nrow mod kAcc
       acc = (int)(nrow & (ws::kAcc - 1));
+      const int b = acc;
       ++nrow;
       if (lane == 0) {
         bool okr = true;
@@ -353,10 +356,14 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
   if (lane == 0) {
     c.stage_info[slot] = make_int4(-1, 0, 0, 0);
     mbar_arrive_cnt(&c.full[slot], ws::kFullCount);
-    // end markers for both solver warpgroups
-    for (int bb = 0; bb < 2; ++bb) {
-      if (row_used & (1u << bb))
+    // end markers: rows nrow .. nrow + NG - 1, the next row of each solver warpgroup
+    for (int i = 0; i < NG; ++i) {
+      const int bb = (int)((nrow + i) & (ws::kAcc - 1));
+      if (row_used & (1u << bb)) {
         tc::mbar_wait_or_abort(&c.row_empty[bb], (row_par >> bb) & 1, c.misc + 1);
+        row_par ^= 1u << bb;
+      }
+      row_used |= 1u << bb;
       c.row_info[bb] = make_int4(-1, 0, 0, 0);
       tc::mbar_arrive(&c.row_full[bb]);
     }
@@ -433,6 +440,17 @@ __device__ __forceinline__ float matvec_tmem(uint32_t tA, const float *v, float 
     }
   }
   return (q0 + q1) + (q2 + q3);
+}
+
+// Sum of one per-thread value over the warpgroup: one barrier.
+__device__ __forceinline__ float group_sum1(float a, float *red, int &slot, const Bar &B) {
+  a = warp_sum(a);
+  float *r = red + slot * 16;
+  if ((B.tid & 31) == 0) r[B.tid >> 5] = a;
+  B.sync();
+  const float4 q = *reinterpret_cast<const float4 *>(r);
+  slot ^= 1;
+  return (q.x + q.y) + (q.z + q.w);
 }
 
 // Sum of two per-thread values over the warpgroup: one barrier.
@@ -519,9 +537,9 @@ __device__ __noinline__ int ws_cholesky(float *S, float *dg, float *bv, float *x
 }
 
 // Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA. Row n
-// arrives in row slot n mod 2 (row_info / row_full / row_empty) and
-// accumulator n mod 4, which the group keeps until the row is solved: the
-// CG matrix-vector products read A_u from TMEM.
+// arrives in row slot and accumulator n mod kAcc (the (n / kAcc)-th phase of
+// their barriers); the group keeps the accumulator until the row is solved:
+// the CG matrix-vector products read A_u from TMEM.
 template <int FP, int NP, typename LP, int NG>
 __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &sv,
                          const WsCtrl &c, unsigned char *mem, uint32_t tmem, int wg) {
@@ -531,7 +549,7 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   static_assert(NP <= ws::kBufCols, "the system fits one accumulator");
   const int lt = threadIdx.x & 127, wl = (threadIdx.x >> 5) & 3;
   const Bar B{1 + wg, 128, lt};
-  float *S = reinterpret_cast<float *>(mem);
+  float *S = plan.chol + ((size_t)blockIdx.x * ws::kMaxGroups + wg) * kCholFloats;
   float *dg = reinterpret_cast<float *>(mem + L::oDg), *bv = reinterpret_cast<float *>(mem + L::oBv);
   float *xv = reinterpret_cast<float *>(mem + L::oXv), *tmp = reinterpret_cast<float *>(mem + L::oTmp);
   float *ps = reinterpret_cast<float *>(mem + L::oPs), *red = reinterpret_cast<float *>(mem + L::oRed);
@@ -541,17 +559,16 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   const bool live = m < f;
   ps[lt] = 0.f;  // L::kPs == 128 entries, one per thread
   B.sync();
-  unsigned rpar = 0, apar = 0;  // phase parities: row slots (2 bits), accumulators (4 bits)
   int rslot = 0;
   unsigned long long n_rows = 0, n_ref = 0, n_bad = 0, n_steps = 0, n_fb = 0, n_r0 = 0;
   const uint32_t tlane = tmem + ((uint32_t)(wl * 32) << 16);
   const uint32_t bcol = (uint32_t)(a.ld_src & ~15);
   const int bq = a.ld_src & 15;
   for (long long n = wg;; n += NG) {
-    const int rb = (int)(n & 1), ab = (int)(n & (ws::kAcc - 1));
+    const int rb = (int)(n & (ws::kAcc - 1)), ab = rb;
+    const unsigned par = (unsigned)(n / ws::kAcc) & 1u;
     const uint32_t tA = tlane + (uint32_t)ab * ws::kBufCols;
-    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], (rpar >> rb) & 1u, c.misc + 1);
-    rpar ^= 1u << rb;
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], par, c.misc + 1);
     if (!B.all(ok)) { ws_abort(a, c); break; }
     const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[rb]);
     const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
@@ -562,8 +579,7 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
     const float reg = a.lambda * (float)info.y;
     // the warm start's load overlaps the wait for the accumulator
     float x = (live && sv.x0 && info.z < 0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
-    ok = tc::mbar_wait_or_abort(&c.acc_full[ab], (apar >> ab) & 1u, c.misc + 1);
-    apar ^= 1u << ab;
+    ok = tc::mbar_wait_or_abort(&c.acc_full[ab], par, c.misc + 1);
     if (!B.all(ok)) { ws_abort(a, c); break; }
     tc::tc_fence_after();
     // b_u sits in column c_r = ld of D; rows >= f (no unknown) are ignored
@@ -681,16 +697,16 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
         B.sync();
         float w = matvec_tmem<NP>(tA, ps, reg, p);
         if (!live) w = 0.f;
-        const float pq = group_sum2(p * w, 0.f, red, rslot, B).x;
+        const float pq = group_sum1(p * w, red, rslot, B);
         if (!(pq > 0.f)) break;  // not positive definite along p: fall back
-        const float alpha = gamma / pq;
+        const float alpha = __fdividef(gamma, pq);
         x = fmaf(alpha, p, x);
         r = fmaf(-alpha, w, r);
         z = dinv * r;
         const float2 t = group_sum2(r * z, r * r, red, rslot, B);
         ++it;
         conv = t.y <= target;
-        p = fmaf(t.x / gamma, p, z);
+        p = fmaf(__fdividef(t.x, gamma), p, z);
         gamma = t.x;
       }
       if (lt == 0) n_steps += it;
@@ -764,11 +780,11 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
   c.acc_full = c.empty + ws::NS;
   c.acc_empty = c.acc_full + ws::kAcc;
   c.row_full = c.acc_empty + ws::kAcc;
-  c.row_empty = c.row_full + 2;
-  c.drain = c.row_empty + 2;
+  c.row_empty = c.row_full + ws::kAcc;
+  c.drain = c.row_empty + ws::kAcc;
   c.stage_info = reinterpret_cast<int4 *>(ctrl + L::kBars);
   c.row_info = c.stage_info + ws::NS;
-  c.misc = reinterpret_cast<volatile int *>(c.row_info + 2);
+  c.misc = reinterpret_cast<volatile int *>(c.row_info + ws::kAcc);
   const int tid = threadIdx.x, warp = tid >> 5;
 
   if (tid == 0) {
@@ -779,8 +795,6 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
     for (int b = 0; b < ws::kAcc; ++b) {
       tc::mbar_init(&c.acc_full[b], 1);
       tc::mbar_init(&c.acc_empty[b], 128);
-    }
-    for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&c.row_full[b], 1);
       tc::mbar_init(&c.row_empty[b], 1);
     }
@@ -807,7 +821,7 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
     if ((tid & 31) == 0) ws_mma(a, c, base, tmem, idesc);
     __syncwarp();
   } else if (warp == ws::prod_warp<NG>()) {
-    ws_produce<LP>(a, plan, g, c, base, base + L::oRing, n_empty);
+    ws_produce<LP, NG>(a, plan, g, c, base, base + L::oRing, n_empty);
     if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
   } else if (warp < 4 * NG) {
     ws_solve<FP, NP, LP, NG>(a, plan, sv, c, base + L::oSolver + (size_t)(warp >> 2) * L::kSolver,
@@ -837,8 +851,9 @@ static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
   auto kern = rows_tc_ws_kernel<FP, NP, LP, NG>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kTotal);
   if (err != cudaSuccess) return err;
-  int64_t grid = num_sms;
+  int64_t grid = std::min(num_sms, plan.ctas);
   if (grid > plan.nitems) grid = plan.nitems > 0 ? plan.nitems : 1;
+  if (grid < 1 || !plan.chol) return cudaErrorInvalidValue;
   const int nmma = ((std::max(NP, a.ld_src + 1) + 15) / 16) * 16;  // B columns incl. c_r
   const uint32_t idesc = tc::make_idesc(lp_kind == kLpBf16 ? 1 : 0, nmma);
   kern<<<(unsigned)grid, ws::threads<NG>(), L::kTotal, st>>>(a, idesc, sv, g, plan);
@@ -851,6 +866,9 @@ static cudaError_t launch_ws_np(const RowsArgs &a, int lp_kind, const TcSolve &s
   if (sv.groups == 1)
     return lp_kind == kLpBf16 ? launch_ws<FP, NP, __nv_bfloat16, 1>(a, lp_kind, sv, plan, num_sms, st)
                               : launch_ws<FP, NP, __half, 1>(a, lp_kind, sv, plan, num_sms, st);
+  if (sv.groups == 3)
+    return lp_kind == kLpBf16 ? launch_ws<FP, NP, __nv_bfloat16, 3>(a, lp_kind, sv, plan, num_sms, st)
+                              : launch_ws<FP, NP, __half, 3>(a, lp_kind, sv, plan, num_sms, st);
   return lp_kind == kLpBf16 ? launch_ws<FP, NP, __nv_bfloat16, 2>(a, lp_kind, sv, plan, num_sms, st)
                             : launch_ws<FP, NP, __half, 2>(a, lp_kind, sv, plan, num_sms, st);
 }
@@ -934,7 +952,8 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   const size_t oI = 0, oN = al(sizeof(WorkItem) * items.size()), oB = oN + al(4 * (nh + 1)),
                oC = oB + al(4 * (nh + 1)), oP = oC + al(4 * (nh + 1)),
-               total = oP + al(sizeof(float) * (size_t)slots * 128 * plan->part_ld + 16);
+               oK = oP + al(sizeof(float) * (size_t)slots * 128 * plan->part_ld + 16),
+               total = oK + al(sizeof(float) * (size_t)grid * ws::kMaxGroups * kCholFloats);
   char *d = nullptr;
   if ((e = cudaMalloc(&d, total)) != cudaSuccess) return e;
   e = cudaMemcpyAsync(d + oI, items.data(), sizeof(WorkItem) * items.size(),
@@ -952,6 +971,8 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
   plan->heavy_base = (const int *)(d + oB);
   plan->heavy_count = (unsigned *)(d + oC);
   plan->partial = (float *)(d + oP);
+  plan->chol = (float *)(d + oK);
+  plan->ctas = grid;
   *mem = d;
   return cudaSuccess;
 }

@@ -103,3 +103,37 @@ def test_learned_warm_start_gain_in_als():
     assert r0["mlp"] < 0.5 * r0["zero"]
     for v in rmse.values():
         assert abs(v - rm_ref) / rm_ref < 1e-3
+
+
+@pytest.mark.parametrize("f,prec", [(100, A.PREC_BF16), (16, A.PREC_FP16), (33, A.PREC_BF16),
+                                    (20, A.PREC_FP32)])
+def test_features_match_numpy(f, prec):
+    """Row features [b_u / n_u, diag(A_u) / n_u, log1p(n_u) / 8] against numpy
+    on the same 16-bit (or FP32) factors: empty rows, short rows, rows long
+    enough for several rounds of every warp, and a row long enough to be split
+    across blocks (16-bit path). Tolerance 1e-2 relative (BF16 output)."""
+    rng = np.random.default_rng(5)
+    n = 300
+    deg = np.array([0, 1, 3, 31, 32, 33, 200, 257, 1000, 2600, 0, 17, 20000])
+    ptr = np.zeros(len(deg) + 1, np.int64)
+    ptr[1:] = np.cumsum(deg)
+    col = np.concatenate([rng.choice(n, d, replace=True) for d in deg]).astype(np.int32)
+    val = rng.integers(1, 6, len(col)).astype(np.float32)
+    ld = ((f + 1 + 7) // 8) * 8 if prec != A.PREC_FP32 else f
+    th = np.zeros((n, ld), np.float32)
+    th[:, :f] = rng.standard_normal((n, f)) * 0.3
+    dt = {A.PREC_BF16: torch.bfloat16, A.PREC_FP16: torch.float16, A.PREC_FP32: torch.float32}[prec]
+    src = torch.from_numpy(th).to(dt).cuda()
+    thq = src.float().cpu().numpy().astype(np.float64)[:, :f]
+    ldf = A.Mlp(f, capacity=64).ldf
+    F = A.features(torch.from_numpy(ptr).cuda(), torch.from_numpy(col).cuda(),
+                   torch.from_numpy(val).cuda(), src, f, prec, ldf).float().cpu().numpy()
+    for u in range(len(deg)):
+        s, e = ptr[u], ptr[u + 1]
+        nu = e - s
+        b = (val[s:e, None] * thq[col[s:e]]).sum(0) / max(nu, 1)
+        d = (thq[col[s:e]] ** 2).sum(0) / max(nu, 1)
+        ref = np.concatenate([b, d, [np.log1p(nu) / 8]])
+        got = F[u, :2 * f + 1]
+        assert np.abs(got - ref).max() <= 1e-2 * max(1.0, np.abs(ref).max()), (u, nu)
+        assert not F[u, 2 * f + 1:].any()
