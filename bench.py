@@ -36,7 +36,7 @@ WORKLOAD = "netflix-shape synthetic 480189x17770, ~100.5M ratings (1.4M test), f
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--config", default="netflix")
@@ -82,10 +82,23 @@ class Clocks:
         self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.tmp, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        # wait until the sampler is live; lines written before the timed
+        # region starts are left out of the summary
+        self.skip = 0
+        t0 = time.time()
+        while self.proc and time.time() - t0 < 15:
+            try:
+                n = len(open(self.tmp.name).read().strip().splitlines())
+            except OSError:
+                n = 0
+            if n:
+                self.skip = n
+                break
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *a):
@@ -98,10 +111,12 @@ class Clocks:
 
     def summary(self):
         try:
-            rows = [l.split(",") for l in open(self.tmp.name).read().strip().splitlines()]
+            lines = open(self.tmp.name).read().strip().splitlines()
             os.unlink(self.tmp.name)
         except Exception:
             return None
+        in_region = len(lines) - self.skip
+        rows = [l.split(",") for l in (lines[self.skip:] if in_region > 0 else lines[-1:])]
         rows = [[x.strip() for x in r] for r in rows if len(r) >= 9]
         if not rows:
             return None
@@ -111,7 +126,8 @@ class Clocks:
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         load = sorted(sm)[len(sm) // 2:] if sm else []
         return {"sm_mhz": float(np.median(load)) if load else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows),
+                "samples_in_timed_region": max(0, in_region)}
 
 
 def dist_init(args):

@@ -260,6 +260,9 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
       e = plan_ws(S.ptr, 0, S.rows, M->num_sms, tc_ws_np(f), (int)S.cols, &S.plan, &S.plan_mem, st);
       S.has_plan = e == cudaSuccess;
     }
+    // the autotuner's candidates are loaded now, so no timed launch pays for it
+    for (int g = 2; g <= 3 && e == cudaSuccess && o.solver_groups == 0; ++g)
+      e = prepare_rows_tc_ws(f, kind, g);
     if (e != cudaSuccess) {
       als_model_destroy(M);
       return cuda_fail(e, "als_model_create: work plan");

@@ -31,7 +31,8 @@ struct TcSolve {
   const float *x0;     // CG starting point (m x ld_x0), or null for zero
   int ld_x0;
   int jacobi;          // 1: diagonal preconditioner
-  int groups;          // solver warpgroups per CTA of the warp-specialised kernel (1 or 2)
+  int groups;          // solver warpgroups per CTA of the warp-specialised kernel (1, 2 or 3)
+  int prepare;         // 1: only load the kernel instance and set its attributes
 };
 
 // Work list of the warp-specialised kernel, planned on the host per side:
@@ -72,6 +73,7 @@ bool tc_ws_supported(int f);
 cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
                               const WsPlan &plan, int num_sms, cudaStream_t st);
 int tc_ws_np(int f);
+cudaError_t prepare_rows_tc_ws(int f, int lp_kind, int groups);
 
 // Degree-binned visiting order: rows sorted by descending floor(log2(degree)).
 // work: 3 * kOrderBins unsigned ints of device scratch.

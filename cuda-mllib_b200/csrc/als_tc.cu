@@ -394,7 +394,7 @@ cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_ma
   if (a.ld_src != tc_padded_ld(a.f) || !a.error) return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
   TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst, cg_jacobi,
-             groups >= 1 && groups <= 3 ? groups : 2};
+             groups >= 1 && groups <= 3 ? groups : 2, 0};
   if (plan && tc_ws_supported(a.f)) return launch_rows_tc_ws(a, lp_kind, sv, *plan, num_sms, st);
   const int f = a.f, np = tc_geom(f).np;
   // (FP, NP): FP >= f is the Cholesky tile extent, NP = roundup16(f + 1) the MMA N

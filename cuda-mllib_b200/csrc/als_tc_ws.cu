@@ -7,29 +7,30 @@
 // global slots; the chunk that finishes last sums them in chunk order and
 // solves the row.
 //
-//   warp 8      producer: per stage of 64 ratings, 16-byte cp.async copies of
-//               the rated factor rows (half a warp per row, one 16-byte piece
-//               per lane) into a 128B-swizzled MN-major tile, the swizzle
-//               computed in the destination address; rows past the stage are
-//               zero-filled. The lanes also write r_uk into tile column
-//               c_r = ld (a pad column the copies never touch). Completion
-//               reaches the MMA thread through
+//   warps 4NG,  two producers, taking alternate stages of 64 ratings: 16-byte
+//   4NG+2       cp.async copies of the rated factor rows (half a warp per row,
+//               one 16-byte piece per lane) into a 128B-swizzled MN-major
+//               tile, the swizzle computed in the destination address; rows
+//               past the item's end are zero-filled. The lanes also write r_uk
+//               into tile column c_r = ld (a pad column the copies never
+//               touch). Completion reaches the MMA thread through
 //               cp.async.mbarrier.arrive. Column indices and ratings arrive
-//               DI - 1 stages ahead through a cp.async ring in shared memory,
-//               item metadata 32 items at a time, so no dependent global load
-//               is on the critical path.
-//   warp 9      MMA issuer (one thread): per stage, tcgen05.mma kind::f16,
+//               DI - 1 owned stages ahead through a per-producer cp.async ring
+//               in shared memory, item metadata 32 items at a time, so no
+//               dependent global load is on the critical path.
+//   warp 4NG+1  MMA issuer (one thread): per stage, tcgen05.mma kind::f16,
 //               A = tile^T (M = 128), B = the first N = roundup16(max(NP,
-//               c_r + 1)) tile columns, into one of two TMEM accumulators
-//               (rows alternate); tcgen05.commit frees the stage and, after
-//               the item's last stage, marks the accumulator full.
-//               D[:f, :f] = sum theta theta^T, D[:f, c_r] = b_u; the other
-//               columns below c_r are zero, rows >= f are ignored.
-//   warps 0-3,  two solver warpgroups, one per accumulator: read D with
-//   4-7         tcgen05.ld (thread m <- TMEM lane m = row m of A_u), release
-//               it, then CG in registers (optionally Jacobi-preconditioned;
-//               Cholesky fallback) or the register-tile Cholesky + FP64-residual
-//               refinement, each on its own named barrier.
+//               c_r + 1)) tile columns, into TMEM accumulator r mod 4 for row
+//               r; tcgen05.commit frees the stage and, after the item's last
+//               stage, marks the accumulator full. D[:f, :f] = sum theta
+//               theta^T, D[:f, c_r] = b_u; the other columns below c_r are
+//               zero, rows >= f are ignored.
+//   warps 0 ..  NG solver warpgroups (rows r = g mod NG to group g): read b_u
+//   4NG-1       with tcgen05.ld (thread m <- TMEM lane m = row m of A_u) and
+//               keep the accumulator for the whole solve: CG whose products
+//               read A_u from TMEM (warm start optimally scaled; Cholesky
+//               fallback), or the register-tile Cholesky + FP64-residual
+//               refinement, each group on its own named barrier.
 //
 // Every mbarrier wait is bounded and gives up when another role aborted; a
 // timeout sets the error word and all roles leave their loops.
@@ -37,6 +38,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "als_common.cuh"
@@ -46,11 +48,11 @@
 namespace als {
 
 namespace ws {
-// NG solver warpgroups (warps 0 .. 4 NG - 1), then the producer and MMA warps.
-// Registers per thread are capped by the busiest SM sub-partition: 255 with
-// NG = 1 (two warps), 168 with NG = 2 (three), 128 with NG = 3 (four).
-template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG + 64; }
-template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }
+// NG solver warpgroups (warps 0 .. 4 NG - 1), then producer 0, the MMA warp
+// and producer 1. Registers per thread are capped by the busiest SM
+// sub-partition: 168 with NG = 1 or 2 (three warps), 128 with NG = 3 (four).
+template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG + 96; }
+template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }  // and 4 NG + 2
 template <int NG> __host__ __device__ constexpr int mma_warp() { return 4 * NG + 1; }
 constexpr int NS = 6;                             // shared-memory stages
 constexpr int KS = 64;                            // ratings per stage
@@ -58,24 +60,47 @@ constexpr int kAtom = (KS / 8) * 1024;            // one 64-element MN atom of a
 constexpr int kStageBytes = 2 * kAtom;            // tile columns 0-63 and 64-127
 constexpr int kAcc = 4;                           // TMEM accumulators (row n -> n mod 4)
 constexpr int kMaxGroups = 3;                     // solver warpgroups per CTA at most
+// Row hand-over slots: kGroupSlots per solver warpgroup. Row n goes to group
+// n mod NG, the k-th row of a group (k = n / NG) to its slot k mod
+// kGroupSlots, as that slot's (k / kGroupSlots)-th barrier phase. An mbarrier
+// parity wait tells only the current and the preceding phase apart, so no
+// wait may name a phase two ahead of its barrier's:
+//  - a group waits only on its own slots, in its own order;
+//  - a producer posting row r waits for the slot's previous row, r - 8 NG,
+//    to have been taken; when it can post row r, the MMA has taken stage
+//    (first stage of r) - NS and so started row >= r - NS, hence rows up to
+//    r - NS - kAcc = r - 10 are solved and their successors' rows taken, and
+//    r - 16 NG (two slot uses back) is long taken.
+constexpr int kGroupSlots = 8;
+constexpr int kRowSlots = kGroupSlots * kMaxGroups;
+template <int NG> __host__ __device__ constexpr int row_slot(long long n) {
+  return (int)(n % NG) * kGroupSlots + (int)((n / NG) % kGroupSlots);
+}
+template <int NG> __host__ __device__ constexpr unsigned row_parity(long long n) {
+  return (unsigned)((n / NG) / kGroupSlots) & 1u;
+}
 constexpr int kBufCols = 128;                     // TMEM columns per accumulator
 constexpr int kTmemCols = kAcc * kBufCols;        // all 512 columns
 constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
 constexpr int DI = 8;                             // index-ring slots (stages fetched ahead + 1)
-constexpr int kRingSlot = 8 * KS + 32;            // column indices, ratings, two int4 of header
+constexpr int kRingSlot = 8 * KS + 48;            // column indices, ratings, three int4 of header
+constexpr int kProducers = 2;                     // producer warps, taking alternate stages
 }  // namespace ws
 
 struct WsGeom {
   int nj;  // 16-byte pieces per factor row (ld_src / 8, at most 16)
 };
 
-// Per solver warpgroup: vectors of the fallback Cholesky (its f x f tile lives
-// in global scratch, plan.chol), the CG broadcast vector and reduction slots.
-template <int FP, int NP, int NG>
-struct WsLayout {
+// Per solver warpgroup: the fallback Cholesky's tile when shared memory has
+// room for it (else the tile lives in global scratch, plan.chol) and vectors,
+// the CG broadcast vector and reduction slots.
+template <int FP, int NP, int NG, bool SIN>
+struct WsLayoutT {
   static constexpr int LDS = FP + 1;
   static_assert((size_t)FP * LDS <= (size_t)kCholFloats, "Cholesky tile fits its scratch");
-  static constexpr size_t oDg = 0, oBv = oDg + FP * 4, oXv = oBv + FP * 4, oTmp = oXv + FP * 4;
+  static constexpr bool kSInSmem = SIN;
+  static constexpr size_t kS = SIN ? (size_t)FP * LDS * 4 : 0;
+  static constexpr size_t oDg = kS, oBv = oDg + FP * 4, oXv = oBv + FP * 4, oTmp = oXv + FP * 4;
   static constexpr size_t oPs = (oTmp + FP * 4 + 15) / 16 * 16;
   static constexpr int kPs = 128;  // CG broadcast vector: one entry per thread of the warpgroup
   static_assert(NP <= kPs, "the broadcast vector covers every accumulator column");
@@ -85,16 +110,20 @@ struct WsLayout {
   static constexpr size_t kSolver = (oMisc + 16 + 127) / 128 * 128;
   static constexpr size_t oSolver = (size_t)ws::NS * ws::kStageBytes;
   static constexpr size_t oCtrl = oSolver + NG * kSolver;
-  // full, empty per stage; acc_full, acc_empty, row_full, row_empty per
-  // accumulator (row n uses accumulator and row slot n mod kAcc); drain; one
+  // full, empty per stage; acc_full, acc_empty per accumulator (row n uses
+  // accumulator n mod kAcc); row_full, row_empty per row slot; drain; one
   // spare (16-byte multiple)
-  static constexpr size_t kBars = 8 * (2 * ws::NS + 4 * ws::kAcc + 2);
-  static constexpr size_t kCtrl = kBars + 16 * (ws::NS + ws::kAcc) + 16;
+  static constexpr size_t kBars = 8 * (2 * ws::NS + 2 * ws::kAcc + 2 * ws::kRowSlots + 2);
+  static constexpr size_t kCtrl = kBars + 16 * (ws::NS + ws::kRowSlots) + 16;
   static constexpr size_t oRing = oCtrl + kCtrl;  // 16-byte aligned
-  static constexpr size_t kTotal = 1024 + oRing + (size_t)ws::DI * ws::kRingSlot;
+  static constexpr size_t kTotal = 1024 + oRing + (size_t)ws::kProducers * ws::DI * ws::kRingSlot;
   static_assert(kCtrl % 16 == 0 && ws::kRingSlot % 16 == 0, "ring alignment");
-  static_assert(kTotal <= 232448, "227 KB of shared memory per CTA");
 };
+
+template <int FP, int NP, int NG>
+using WsLayout = typename std::conditional<WsLayoutT<FP, NP, NG, true>::kTotal <= 232448,
+                                           WsLayoutT<FP, NP, NG, true>,
+                                           WsLayoutT<FP, NP, NG, false>>::type;
 
 struct WsCtrl {
   uint64_t *full, *empty, *acc_full, *acc_empty, *row_full, *row_empty, *drain;
@@ -150,10 +179,11 @@ __device__ __forceinline__ void cp_async4(uint32_t dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
 }
 
-// Fetch cursor of the producer warp: walks the CTA's items stage by stage,
-// ws::DI - 1 stages ahead of the stage being issued, and copies each stage's
-// column indices and ratings into a shared-memory ring with cp.async (one
-// commit group per stage). Rows without ratings are finished here (x_u = 0).
+// Fetch cursor of a producer warp: walks the CTA's items stage by stage (the
+// global stage sequence every producer sees alike) and copies the column
+// indices and ratings of the stages it owns into its shared-memory ring with
+// cp.async (one commit group per owned stage). Rows without ratings are
+// finished by the cursor of producer 0 (x_u = 0).
 template <typename LP>
 struct FetchCursor {
   ItemBatch cb, nb;
@@ -161,6 +191,9 @@ struct FetchCursor {
   int bpos;
   long long s, e, k0;
   int u, deg, part, heavy;
+  int row;  // rows with ratings before the current item
+  int gs;   // global index of the current stage
+  bool owner;
 
   __device__ __forceinline__ void extract() {
     s = ((long long)__shfl_sync(0xffffffffu, cb.lo.y, bpos) << 32) |
@@ -185,31 +218,49 @@ struct FetchCursor {
   __device__ __forceinline__ void settle(const RowsArgs &a, const WsPlan &p, int lane,
                                          unsigned long long &n_empty) {
     while (u >= 0 && e == s) {
-      for (int i = lane; i < a.f; i += 32) {
-        a.dst[(long long)u * a.ld_dst + i] = 0.f;
-        if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[(long long)u * a.ld_dst_lp + i] = LP(0.f);
-      }
-      if (lane == 0) {
-        if (a.row_flags) a.row_flags[u] = kRowEmpty;
-        ++n_empty;
+      if (owner) {
+        for (int i = lane; i < a.f; i += 32) {
+          a.dst[(long long)u * a.ld_dst + i] = 0.f;
+          if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[(long long)u * a.ld_dst_lp + i] = LP(0.f);
+        }
+        if (lane == 0) {
+          if (a.row_flags) a.row_flags[u] = kRowEmpty;
+          ++n_empty;
+        }
       }
       next_item(p, lane);
     }
     k0 = s;
   }
-  __device__ __forceinline__ void init(const RowsArgs &a, const WsPlan &p, int lane,
+  __device__ __forceinline__ void init(const RowsArgs &a, const WsPlan &p, int lane, bool own,
                                        unsigned long long &n_empty) {
+    owner = own;
     bi = 0;
     bpos = 0;
+    row = 0;
+    gs = 0;
     cb = load_batch(p, 0, lane);
     nb = load_batch(p, 1, lane);
     extract();
     settle(a, p, lane, n_empty);
   }
-  // copies of stage `seq` into ring slot seq mod DI; an invalid header past the end
-  __device__ __forceinline__ void fetch(const RowsArgs &a, const WsPlan &p, unsigned char *ring,
-                                        long long seq, int lane, unsigned long long &n_empty) {
-    unsigned char *rs = ring + (int)(seq % ws::DI) * ws::kRingSlot;
+  // move to the next global stage
+  __device__ __forceinline__ void advance(const RowsArgs &a, const WsPlan &p, int lane,
+                                          unsigned long long &n_empty) {
+    if (u < 0) return;
+    ++gs;
+    k0 += ws::KS;
+    if (k0 >= e) {
+      next_item(p, lane);
+      settle(a, p, lane, n_empty);
+      ++row;
+    }
+  }
+  // copies of the current stage into ring slot rs, and its header: {u, deg,
+  // part, heavy}, {kc, first, last, valid}, {row, stage}; past the end the
+  // header is invalid and carries the number of rows and stages
+  __device__ __forceinline__ void fetch(const RowsArgs &a, unsigned char *rs, int lane) {
+    int4 *h = reinterpret_cast<int4 *>(rs + 8 * ws::KS);
     if (u >= 0) {
       const int kc = (int)(e - k0 < ws::KS ? e - k0 : ws::KS);
       const uint32_t r0 = tc::smem_u32(rs);
@@ -222,17 +273,13 @@ struct FetchCursor {
         }
       }
       if (lane == 0) {
-        int4 *h = reinterpret_cast<int4 *>(rs + 8 * ws::KS);
         h[0] = make_int4(u, deg, part, heavy);
         h[1] = make_int4(kc, k0 == s ? 1 : 0, k0 + ws::KS >= e ? 1 : 0, 1);
-      }
-      k0 += ws::KS;
-      if (k0 >= e) {
-        next_item(p, lane);
-        settle(a, p, lane, n_empty);
+        h[2] = make_int4(row, gs, 0, 0);
       }
     } else if (lane == 0) {
-      reinterpret_cast<int4 *>(rs + 8 * ws::KS)[1] = make_int4(0, 0, 0, 0);
+      h[1] = make_int4(0, 0, 0, 0);
+      h[2] = make_int4(row, gs, 0, 0);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
@@ -285,50 +332,70 @@ __device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &pl
   }
 }
 
+// Producer k of ws::kProducers owns global stages k, k + kProducers, ...;
+// stage t of the sequence goes to shared-memory stage t mod NS (the
+// (t / NS)-th phase of its barriers), row r to row slot and accumulator
+// r mod kAcc and to row slot row_slot<NG>(r), so the producers need no
+// coordination beyond those barriers.
+// The producer that owns the stage just past the last one writes the end
+// markers.
 template <typename LP, int NG>
 __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &g,
-                           const WsCtrl &c, unsigned char *stages, unsigned char *ring,
+                           const WsCtrl &c, unsigned char *stages, unsigned char *ring, int k,
                            unsigned long long &n_empty_rows) {
+  constexpr int P = ws::kProducers;
   const int lane = threadIdx.x & 31;
   const uint32_t st0 = tc::smem_u32(stages);
-  unsigned empty_par = 0, empty_used = 0, row_par = 0, row_used = 0;
-  int slot = 0, acc = 0;
-  long long nrow = 0;
   FetchCursor<LP> fc;
-  fc.init(a, plan, lane, n_empty_rows);
-  for (int q = 0; q < ws::DI - 1; ++q) fc.fetch(a, plan, ring, q, lane, n_empty_rows);
-  for (long long n = 0;; ++n) {
-    fc.fetch(a, plan, ring, n + ws::DI - 1, lane, n_empty_rows);
+  fc.init(a, plan, lane, k == 0, n_empty_rows);
+  for (int i = 0; i < k; ++i) fc.advance(a, plan, lane, n_empty_rows);
+  auto fetch_next = [&](long long t) {
+    fc.fetch(a, ring + (int)(t % ws::DI) * ws::kRingSlot, lane);
+    for (int i = 0; i < P; ++i) fc.advance(a, plan, lane, n_empty_rows);
+  };
+  for (int q = 0; q < ws::DI - 1; ++q) fetch_next(q);
+  bool ends = false;
+  int end_rows = 0, end_stage = 0;
+  for (long long t = 0;; ++t) {
+    fetch_next(t + ws::DI - 1);
     asm volatile("cp.async.wait_group %0;" ::"n"(ws::DI - 1) : "memory");
     __syncwarp();
-    const unsigned char *rs = ring + (int)(n % ws::DI) * ws::kRingSlot;
-    const int4 h1 = reinterpret_cast<const int4 *>(rs + 8 * ws::KS)[1];
-    if (__any_sync(0xffffffffu, h1.w == 0 || c.misc[1] != 0)) break;  // warp-uniform exit
+    const unsigned char *rs = ring + (int)(t % ws::DI) * ws::kRingSlot;
+    const int4 *hd = reinterpret_cast<const int4 *>(rs + 8 * ws::KS);
+    const int4 h1 = hd[1], h2 = hd[2];
+    if (__any_sync(0xffffffffu, h1.w == 0 || c.misc[1] != 0)) {  // warp-uniform exit
+      ends = h1.w == 0 && c.misc[1] == 0 && h2.y == (int)(P * t + k);
+      end_rows = h2.x;
+      end_stage = h2.y;
+      break;
+    }
     const int kc = h1.x, first = h1.y, last = h1.z;
+    const int st = (int)(P * t + k), slot = st % ws::NS;
+    if (h2.y != st) {  // the cursors disagree: give up rather than mix up stages
+      if (lane == 0) ws_abort(a, c);
+      __syncwarp();
+      break;
+    }
+    // every stage of row h2.x accumulates into accumulator h2.x mod kAcc, whichever
+    // producer took the row's first stage
+    const int acc = h2.x & (ws::kAcc - 1);
     if (first) {
-      // row nrow: row slot and accumulator nrow mod kAcc
-      acc = (int)(nrow & (ws::kAcc - 1));
-      const int b = acc;
-      ++nrow;
+      // the row's first stage also hands row h2.x to its solver group
+      const int r = h2.x, rs2 = ws::row_slot<NG>(r);
       if (lane == 0) {
         bool okr = true;
-        if (row_used & (1u << b)) {
-          okr = tc::mbar_wait_or_abort(&c.row_empty[b], (row_par >> b) & 1, c.misc + 1);
-          row_par ^= 1u << b;
-        }
-        row_used |= 1u << b;
+        if (r >= ws::kGroupSlots * NG)  // the slot's previous row has been taken
+          okr = tc::mbar_wait_or_abort(&c.row_empty[rs2],
+                                       ws::row_parity<NG>(r - ws::kGroupSlots * NG), c.misc + 1);
         if (!okr) c.misc[1] = 1;
-        c.row_info[b] = reinterpret_cast<const int4 *>(rs + 8 * ws::KS)[0];
-        tc::mbar_arrive(&c.row_full[b]);
+        c.row_info[rs2] = hd[0];
+        tc::mbar_arrive(&c.row_full[rs2]);
       }
     }
     const int krows = (kc + 15) & ~15;
     bool okw = true;
-    if (empty_used & (1u << slot)) {
-      okw = tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
-      empty_par ^= 1u << slot;
-    }
-    empty_used |= 1u << slot;
+    if (st >= ws::NS)
+      okw = tc::mbar_wait_or_abort(&c.empty[slot], (unsigned)((st / ws::NS) - 1) & 1u, c.misc + 1);
     if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
     const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
     if (lane == 0) c.stage_info[slot] = make_int4(acc, krows / 16, first, last);
@@ -338,32 +405,31 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     // elements stay zero
     const float *vr = reinterpret_cast<const float *>(rs + 4 * ws::KS);
     const uint32_t rbase = sa + (uint32_t)(g.nj >> 3) * ws::kAtom, rch = (uint32_t)(g.nj & 7);
-    for (int k = lane; k < krows; k += 32) {
-      const uint16_t w = k < kc ? tc::to_bits<LP>(vr[k]) : (uint16_t)0;
-      const uint32_t dst = rbase + (k >> 3) * 1024 + (k & 7) * 128 + ((rch ^ (uint32_t)(k & 7)) << 4);
+    for (int kk = lane; kk < krows; kk += 32) {
+      const uint16_t w = kk < kc ? tc::to_bits<LP>(vr[kk]) : (uint16_t)0;
+      const uint32_t dst = rbase + (kk >> 3) * 1024 + (kk & 7) * 128 + ((rch ^ (uint32_t)(kk & 7)) << 4);
       asm volatile("st.shared.u16 [%0], %1;" ::"r"(dst), "h"(w));
     }
     tc::fence_proxy_async();             // the rating stores, for the tensor core
     tc::cp_async_arrive(&c.full[slot]);  // once this lane's copies have landed
     __syncwarp();
     if (lane == 0) tc::mbar_arrive(&c.full[slot]);  // releases the rating stores
-    slot = slot + 1 == ws::NS ? 0 : slot + 1;
   }
   asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into the ring outlives the warp
-  // end marker for the MMA thread
-  if (empty_used & (1u << slot))
-    tc::mbar_wait_or_abort(&c.empty[slot], (empty_par >> slot) & 1, c.misc + 1);
+  if (!ends) return;
+  // end marker for the MMA thread at stage end_stage
+  const int slot = end_stage % ws::NS;
+  if (end_stage >= ws::NS)
+    tc::mbar_wait_or_abort(&c.empty[slot], (unsigned)((end_stage / ws::NS) - 1) & 1u, c.misc + 1);
   if (lane == 0) {
     c.stage_info[slot] = make_int4(-1, 0, 0, 0);
     mbar_arrive_cnt(&c.full[slot], ws::kFullCount);
-    // end markers: rows nrow .. nrow + NG - 1, the next row of each solver warpgroup
+    // end markers: rows end_rows .. end_rows + NG - 1, the next row of each solver warpgroup
     for (int i = 0; i < NG; ++i) {
-      const int bb = (int)((nrow + i) & (ws::kAcc - 1));
-      if (row_used & (1u << bb)) {
-        tc::mbar_wait_or_abort(&c.row_empty[bb], (row_par >> bb) & 1, c.misc + 1);
-        row_par ^= 1u << bb;
-      }
-      row_used |= 1u << bb;
+      const int r = end_rows + i, bb = ws::row_slot<NG>(r);
+      if (r >= ws::kGroupSlots * NG)
+        tc::mbar_wait_or_abort(&c.row_empty[bb], ws::row_parity<NG>(r - ws::kGroupSlots * NG),
+                               c.misc + 1);
       c.row_info[bb] = make_int4(-1, 0, 0, 0);
       tc::mbar_arrive(&c.row_full[bb]);
     }
@@ -537,8 +603,8 @@ __device__ __noinline__ int ws_cholesky(float *S, float *dg, float *bv, float *x
 }
 
 // Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA. Row n
-// arrives in row slot and accumulator n mod kAcc (the (n / kAcc)-th phase of
-// their barriers); the group keeps the accumulator until the row is solved:
+// arrives in row slot row_slot<NG>(n) and accumulator n mod kAcc (the
+// (n / kAcc)-th phase of its barriers); the group keeps the accumulator until the row is solved:
 // the CG matrix-vector products read A_u from TMEM.
 template <int FP, int NP, typename LP, int NG>
 __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &sv,
@@ -549,7 +615,8 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   static_assert(NP <= ws::kBufCols, "the system fits one accumulator");
   const int lt = threadIdx.x & 127, wl = (threadIdx.x >> 5) & 3;
   const Bar B{1 + wg, 128, lt};
-  float *S = plan.chol + ((size_t)blockIdx.x * ws::kMaxGroups + wg) * kCholFloats;
+  float *S = L::kSInSmem ? reinterpret_cast<float *>(mem)
+                         : plan.chol + ((size_t)blockIdx.x * ws::kMaxGroups + wg) * kCholFloats;
   float *dg = reinterpret_cast<float *>(mem + L::oDg), *bv = reinterpret_cast<float *>(mem + L::oBv);
   float *xv = reinterpret_cast<float *>(mem + L::oXv), *tmp = reinterpret_cast<float *>(mem + L::oTmp);
   float *ps = reinterpret_cast<float *>(mem + L::oPs), *red = reinterpret_cast<float *>(mem + L::oRed);
@@ -565,10 +632,10 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   const uint32_t bcol = (uint32_t)(a.ld_src & ~15);
   const int bq = a.ld_src & 15;
   for (long long n = wg;; n += NG) {
-    const int rb = (int)(n & (ws::kAcc - 1)), ab = rb;
+    const int rb = ws::row_slot<NG>(n), ab = (int)(n & (ws::kAcc - 1));
     const unsigned par = (unsigned)(n / ws::kAcc) & 1u;
     const uint32_t tA = tlane + (uint32_t)ab * ws::kBufCols;
-    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], par, c.misc + 1);
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], ws::row_parity<NG>(n), c.misc + 1);
     if (!B.all(ok)) { ws_abort(a, c); break; }
     const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[rb]);
     const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
@@ -780,11 +847,11 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
   c.acc_full = c.empty + ws::NS;
   c.acc_empty = c.acc_full + ws::kAcc;
   c.row_full = c.acc_empty + ws::kAcc;
-  c.row_empty = c.row_full + ws::kAcc;
-  c.drain = c.row_empty + ws::kAcc;
+  c.row_empty = c.row_full + ws::kRowSlots;
+  c.drain = c.row_empty + ws::kRowSlots;
   c.stage_info = reinterpret_cast<int4 *>(ctrl + L::kBars);
   c.row_info = c.stage_info + ws::NS;
-  c.misc = reinterpret_cast<volatile int *>(c.row_info + ws::kAcc);
+  c.misc = reinterpret_cast<volatile int *>(c.row_info + ws::kRowSlots);
   const int tid = threadIdx.x, warp = tid >> 5;
 
   if (tid == 0) {
@@ -795,6 +862,8 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
     for (int b = 0; b < ws::kAcc; ++b) {
       tc::mbar_init(&c.acc_full[b], 1);
       tc::mbar_init(&c.acc_empty[b], 128);
+    }
+    for (int b = 0; b < ws::kRowSlots; ++b) {
       tc::mbar_init(&c.row_full[b], 1);
       tc::mbar_init(&c.row_empty[b], 1);
     }
@@ -820,8 +889,10 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
   if (warp == ws::mma_warp<NG>()) {
     if ((tid & 31) == 0) ws_mma(a, c, base, tmem, idesc);
     __syncwarp();
-  } else if (warp == ws::prod_warp<NG>()) {
-    ws_produce<LP, NG>(a, plan, g, c, base, base + L::oRing, n_empty);
+  } else if (warp == ws::prod_warp<NG>() || warp == ws::prod_warp<NG>() + 2) {
+    const int k = warp == ws::prod_warp<NG>() ? 0 : 1;
+    ws_produce<LP, NG>(a, plan, g, c, base, base + L::oRing + (size_t)k * ws::DI * ws::kRingSlot, k,
+                       n_empty);
     if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
   } else if (warp < 4 * NG) {
     ws_solve<FP, NP, LP, NG>(a, plan, sv, c, base + L::oSolver + (size_t)(warp >> 2) * L::kSolver,
@@ -837,12 +908,30 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
 }
 
 bool tc_ws_supported(int f) { return f >= 16 && f <= 112; }
+
+// Load the kernel instance for (f, lp_kind, groups) and set its shared-memory
+// attribute without launching it, so that its first real launch (for example
+// one the autotuner times) carries no loading cost.
+cudaError_t prepare_rows_tc_ws(int f, int lp_kind, int groups) {
+  RowsArgs a{};
+  a.f = f;
+  a.ld_src = tc_padded_ld(f);
+  a.src = reinterpret_cast<const void *>(uintptr_t(256));  // never dereferenced
+  TcSolve sv{};
+  sv.groups = groups;
+  sv.prepare = 1;
+  WsPlan plan;
+  plan.nitems = 1;
+  plan.part_ld = 132;
+  return launch_rows_tc_ws(a, lp_kind, sv, plan, 1, 0);
+}
 int tc_ws_np(int f) { return ((f + 15) / 16) * 16; }
 
 template <int FP, int NP, typename LP, int NG>
 static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
                              const WsPlan &plan, int num_sms, cudaStream_t st) {
   using L = WsLayout<FP, NP, NG>;
+  static_assert(L::kTotal <= 232448, "227 KB of shared memory per CTA");
   WsGeom g;
   g.nj = a.ld_src / 8;
   if (a.ld_src % 8 != 0 || a.ld_src > 120 || NP < a.f || FP < a.f || plan.part_ld < NP + 1)
@@ -850,7 +939,7 @@ static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
   auto kern = rows_tc_ws_kernel<FP, NP, LP, NG>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kTotal);
-  if (err != cudaSuccess) return err;
+  if (err != cudaSuccess || sv.prepare) return err;
   int64_t grid = std::min(num_sms, plan.ctas);
   if (grid > plan.nitems) grid = plan.nitems > 0 ? plan.nitems : 1;
   if (grid < 1 || !plan.chol) return cudaErrorInvalidValue;
@@ -945,9 +1034,21 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
       items.push_back(w);
     }
   }
-  std::stable_sort(items.begin(), items.end(), [](const WorkItem &x, const WorkItem &y) {
-    return x.e - x.s > y.e - y.s;
-  });
+  // largest first, ties in row order: a stable counting sort on the item size
+  // (at most `split` ratings), linear in the number of rows
+  {
+    std::vector<int64_t> start((size_t)split + 2, 0);
+    for (const WorkItem &w : items) ++start[(size_t)(split - (w.e - w.s))];
+    int64_t acc = 0;
+    for (auto &v : start) {
+      const int64_t c = v;
+      v = acc;
+      acc += c;
+    }
+    std::vector<WorkItem> sorted(items.size());
+    for (const WorkItem &w : items) sorted[(size_t)start[(size_t)(split - (w.e - w.s))]++] = w;
+    items.swap(sorted);
+  }
   const size_t nh = hn.size();
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   const size_t oI = 0, oN = al(sizeof(WorkItem) * items.size()), oB = oN + al(4 * (nh + 1)),
