@@ -751,7 +751,11 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       }
       if (!live) r = 0.f;
       float z = dinv * r;
-      float p = z;
+      // Two barriers per step: z is broadcast through the same barrier that
+      // sums r.z and r.r, and A p is carried by the recurrence
+      // A p_k = A z_k + beta_k A p_{k-1} (p_k = z_k + beta_k p_{k-1}), so the
+      // product is taken of z instead of p.
+      ps[m] = z;
       const float4 t0 = group_sum4(make_float4(r * z, r * r, bm * bm, 0.f), red, rslot, B);
       float gamma = t0.x;
       const float bb = t0.z;
@@ -759,21 +763,23 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       if (lt == 0 && bb > 0.f) n_r0 += (unsigned long long)(1e6f * sqrtf(t0.y / bb));
       bool conv = t0.y <= target;
       int it = 0;
+      float p = 0.f, w = 0.f, beta = 0.f;
       while (!conv && it < sv.cg_max_steps) {
-        ps[m] = p;
-        B.sync();
-        float w = matvec_tmem<NP>(tA, ps, reg, p);
-        if (!live) w = 0.f;
+        float az = matvec_tmem<NP>(tA, ps, reg, z);
+        if (!live) az = 0.f;
+        p = fmaf(beta, p, z);
+        w = fmaf(beta, w, az);
         const float pq = group_sum1(p * w, red, rslot, B);
         if (!(pq > 0.f)) break;  // not positive definite along p: fall back
         const float alpha = __fdividef(gamma, pq);
         x = fmaf(alpha, p, x);
         r = fmaf(-alpha, w, r);
         z = dinv * r;
+        ps[m] = z;  // read by the next product only after the barrier below
         const float2 t = group_sum2(r * z, r * r, red, rslot, B);
         ++it;
         conv = t.y <= target;
-        p = fmaf(__fdividef(t.x, gamma), p, z);
+        beta = __fdividef(t.x, gamma);
         gamma = t.x;
       }
       if (lt == 0) n_steps += it;
