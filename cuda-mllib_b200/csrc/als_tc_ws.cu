@@ -486,10 +486,11 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
 // Row m of (D + diag I) times the broadcast vector v, with row m of D read
 // from TMEM (lane m of accumulator tA) 32 columns at a time: the system stays
 // in TMEM for the whole solve instead of occupying NP registers. Four
-// independent FMA chains.
+// independent FMA chains, carried two to an instruction by the packed FP32
+// FMA of sm_100.
 template <int NP>
 __device__ __forceinline__ float matvec_tmem(uint32_t tA, const float *v, float diag, float vm) {
-  float q0 = diag * vm, q1 = 0.f, q2 = 0.f, q3 = 0.f;
+  float2 q01 = make_float2(diag * vm, 0.f), q23 = make_float2(0.f, 0.f);
 #pragma unroll
   for (int c0 = 0; c0 < NP; c0 += 32) {
     float d[32];
@@ -498,14 +499,12 @@ __device__ __forceinline__ float matvec_tmem(uint32_t tA, const float *v, float 
     for (int k = 0; k < 32; k += 4) {
       if (c0 + k < NP) {
         const float4 p4 = *reinterpret_cast<const float4 *>(v + c0 + k);
-        q0 = fmaf(d[k], p4.x, q0);
-        q1 = fmaf(d[k + 1], p4.y, q1);
-        q2 = fmaf(d[k + 2], p4.z, q2);
-        q3 = fmaf(d[k + 3], p4.w, q3);
+        q01 = __ffma2_rn(make_float2(d[k], d[k + 1]), make_float2(p4.x, p4.y), q01);
+        q23 = __ffma2_rn(make_float2(d[k + 2], d[k + 3]), make_float2(p4.z, p4.w), q23);
       }
     }
   }
-  return (q0 + q1) + (q2 + q3);
+  return (q01.x + q01.y) + (q23.x + q23.y);
 }
 
 // Sum of one per-thread value over the warpgroup: one barrier.

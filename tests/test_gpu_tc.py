@@ -110,3 +110,34 @@ def test_tc_training_rmse_close_to_fp64():
         assert st["kernel_errors"] == 0
         assert abs(rm - rm_ref) / rm_ref < 1e-3, (prec, rm, rm_ref, st)
         M.close()
+
+
+@pytest.mark.parametrize("f", [100, 48])
+def test_solver_groups_agree_with_oracle(f):
+    """The hot kernel with 1, 2 and 3 solver warpgroups (and the autotuner) on
+    a matrix with multi-stage rows and item rows long enough to be split
+    across CTAs: every configuration gives the same bits, and both sides match
+    the FP64 oracle on the BF16-rounded factors (tolerance 1e-3). This covers
+    the two producers' alternate stages and the per-group row hand-over."""
+    r = A.synth(A.scaled_config("netflix", 0.1), seed=7)
+    assert np.diff(r.csc_ptr).max() > 8192  # some item rows are split
+    th = A.init_factors(r.n, f, 11)
+    out = {}
+    for ng in (1, 2, 3, 0):
+        M = A.Model(r, f, A.options(precision=A.PREC_BF16, solver=A.SOLVER_CG,
+                                    warm_start=A.WARM_ZERO, solver_groups=ng), theta0=th)
+        M.half_step(A.SIDE_USERS, 0.05)
+        M.half_step(A.SIDE_ITEMS, 0.05)
+        X, T = (t.cpu().numpy() for t in M.factors())
+        st = M.stats()
+        M.close()
+        assert st["kernel_errors"] == 0, (ng, st)
+        assert st["rows_solved"] == r.m + r.n
+        out[ng] = (X, T)
+    for ng in (2, 3, 0):
+        assert np.array_equal(out[ng][0], out[1][0]) and np.array_equal(out[ng][1], out[1][1]), ng
+    X, T = out[1]
+    Xr, _ = O.half_step(r.csr_ptr, r.csr_col, r.csr_val, rnd(th, A.PREC_BF16), 0.05)
+    assert rel_rows(X, Xr).max() < TOL
+    Tr, _ = O.half_step(r.csc_ptr, r.csc_row, r.csc_val, rnd(X, A.PREC_BF16), 0.05)
+    assert rel_rows(T, Tr).max() < TOL
