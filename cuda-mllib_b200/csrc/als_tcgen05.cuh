@@ -11,7 +11,26 @@ namespace tc {
 
 constexpr int KS = 64;              // items per stage
 constexpr int kStages = 2;
-constexpr unsigned kSpinLimit = 1u << 22;  // try_wait polls (each returns within ~1 us)
+// Every mbarrier wait gives up after kWaitLimitNs of the global timer.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t a, unsigned parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n.reg .pred p;\n"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar);
 
@@ -26,18 +45,12 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
 // Wait until the phase with the given parity has completed. Bounded.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
   const uint32_t a = smem_u32(bar);
-  for (unsigned it = 0; it < kSpinLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n.reg .pred p;\n"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        "selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
+  if (mbar_try_wait(a, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try_wait(a, parity)) return true;
+    if ((it & 63) == 0 && global_ns() - t0 > kWaitLimitNs) return false;
   }
-  return false;
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -59,19 +72,12 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
 __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, unsigned parity,
                                                    volatile int *abort) {
   const uint32_t a = smem_u32(bar);
-  for (unsigned it = 0; it < kSpinLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n.reg .pred p;\n"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        "selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if ((it & 63) == 63 && *abort) return false;
+  if (mbar_try_wait(a, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try_wait(a, parity)) return true;
+    if ((it & 63) == 0 && (*abort || global_ns() - t0 > kWaitLimitNs)) return false;
   }
-  return false;
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
