@@ -399,7 +399,7 @@ def run_engine(args):
                                "theta upload, X download; wall clock; same form (CG from zero)"}
         line["gpu_launches"] += 0
 
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         users, items, Xs, Ts, frac = cpu_sample_plan(r, f, lam, args.cpu_seconds, args.seed)
         dt, fl = cpu_port_step(r, f, lam, users, items, Xs, Ts)
         line["cpu_baseline"] = {"value": round(fl / dt / 1e9, 3), "unit": "GFLOP/s",

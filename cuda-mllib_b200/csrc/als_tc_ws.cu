@@ -484,7 +484,8 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
 // solver warpgroup
 // ---------------------------------------------------------------------------
 // Row m of (D + diag I) times the broadcast vector v, with row m of D read
-// from TMEM (lane m of accumulator tA) 32 columns at a time: the system stays
+// from TMEM (lane m of accumulator tA) 32 columns at a time (64 per wait
+// measured slower): the system stays
 // in TMEM for the whole solve instead of occupying NP registers. Four
 // independent FMA chains, carried two to an instruction by the packed FP32
 // FMA of sm_100.
@@ -1053,6 +1054,22 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
     std::vector<WorkItem> sorted(items.size());
     for (const WorkItem &w : items) sorted[(size_t)start[(size_t)(split - (w.e - w.s))]++] = w;
     items.swap(sorted);
+  }
+  // CTA c takes items c, c + grid, c + 2 grid, ... (balanced by the sort).
+  // Within a CTA the order zigzags between its largest and smallest items,
+  // so rows that load the producers (many ratings) alternate with rows that
+  // load the solvers (few ratings) instead of coming in two long runs.
+  {
+    const int64_t N = (int64_t)items.size(), G = grid;
+    std::vector<WorkItem> zig(items.size());
+    for (int64_t c = 0; c < std::min<int64_t>(G, N); ++c) {
+      const int64_t nc = (N - c + G - 1) / G;
+      for (int64_t j = 0; j < nc; ++j) {
+        const int64_t k = (j & 1) ? nc - 1 - j / 2 : j / 2;
+        zig[(size_t)(c + j * G)] = items[(size_t)(c + k * G)];
+      }
+    }
+    items.swap(zig);
   }
   const size_t nh = hn.size();
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
