@@ -7,8 +7,8 @@
 // global slots; the chunk that finishes last sums them in chunk order and
 // solves the row.
 //
-//   warps 4NG,  two producers, taking alternate stages of 64 ratings: 16-byte
-//   4NG+2       cp.async copies of the rated factor rows (half a warp per row,
+//   warps 4NG,  three producers, taking stages of 64 ratings in turn: 16-byte
+//   4NG+2, +3   cp.async copies of the rated factor rows (half a warp per row,
 //               one 16-byte piece per lane) into a 128B-swizzled MN-major
 //               tile, the swizzle computed in the destination address; rows
 //               past the item's end are zero-filled. The lanes also write r_uk
@@ -49,10 +49,10 @@ namespace als {
 
 namespace ws {
 // NG solver warpgroups (warps 0 .. 4 NG - 1), then producer 0, the MMA warp
-// and producer 1. Registers per thread are capped by the busiest SM
+// and producers 1 and 2. Registers per thread are capped by the busiest SM
 // sub-partition: 168 with NG = 1 or 2 (three warps), 128 with NG = 3 (four).
-template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG + 96; }
-template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }  // and 4 NG + 2
+template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG + 128; }
+template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }  // 4NG+2, 4NG+3 too
 template <int NG> __host__ __device__ constexpr int mma_warp() { return 4 * NG + 1; }
 constexpr int NS = 6;                             // shared-memory stages
 constexpr int KS = 64;                            // ratings per stage
@@ -84,7 +84,8 @@ constexpr int kTmemCols = kAcc * kBufCols;        // all 512 columns
 constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
 constexpr int DI = 8;                             // index-ring slots (stages fetched ahead + 1)
 constexpr int kRingSlot = 8 * KS + 48;            // column indices, ratings, three int4 of header
-constexpr int kProducers = 2;                     // producer warps, taking alternate stages
+constexpr int kProducers = 3;                     // producer warps, taking stages in turn
+static_assert(NS % kProducers == 0, "a stage slot always belongs to the same producer");
 }  // namespace ws
 
 struct WsGeom {
@@ -895,8 +896,8 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
   if (warp == ws::mma_warp<NG>()) {
     if ((tid & 31) == 0) ws_mma(a, c, base, tmem, idesc);
     __syncwarp();
-  } else if (warp == ws::prod_warp<NG>() || warp == ws::prod_warp<NG>() + 2) {
-    const int k = warp == ws::prod_warp<NG>() ? 0 : 1;
+  } else if (warp == ws::prod_warp<NG>() || warp >= ws::prod_warp<NG>() + 2) {
+    const int k = warp == ws::prod_warp<NG>() ? 0 : warp - ws::prod_warp<NG>() - 1;
     ws_produce<LP, NG>(a, plan, g, c, base, base + L::oRing + (size_t)k * ws::DI * ws::kRingSlot, k,
                        n_empty);
     if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
