@@ -331,9 +331,9 @@ def run_engine(args):
     # taken at the x0.25 shape and scaled by the rating count, so only quoted for this workload
     traffic, traffic_src = None, None
     if args.config == "netflix" and args.scale == 1.0 and args.precision in ("bf16", "fp16"):
-        traffic = 1.733e9  # bytes per launch (users 2.092e9, items 1.375e9)
+        traffic = 1.768e9  # bytes per launch (users 2.149e9, items 1.387e9)
         traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum at netflix x0.25, "
-                       "scaled x16.0 by ratings; users 2.092e9, items 1.375e9")
+                       "scaled x16.0 by ratings; users 2.149e9, items 1.387e9")
     roof = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved_gbs / hbm, 4), "traffic": traffic, "traffic_source": traffic_src,
             "peak_kind": f"{src} HBM copy bandwidth",
