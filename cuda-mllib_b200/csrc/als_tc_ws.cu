@@ -456,7 +456,10 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
     const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
     if (info.x < 0) break;
     const int b = info.x, kmma = info.y, first = info.z, last = info.w;
-    tc::fence_proxy_async();  // the producers' copies become visible to the tensor core
+    // No proxy fence here: each producer lane fences its own generic stores of
+    // the ratings before arriving, and the cp.async copies reach the barrier
+    // only once they have landed (the pattern CUTLASS's sm100 cp.async
+    // mainloop uses).
     if (first) {
       if (acc_used & (1u << b)) {
         ok = tc::mbar_wait_or_abort(&c.acc_empty[b], (acc_par >> b) & 1, c.misc + 1);
