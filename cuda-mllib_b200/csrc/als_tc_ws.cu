@@ -523,13 +523,19 @@ __device__ __forceinline__ float group_sum1(float a, float *red, int &slot, cons
   return (q.x + q.y) + (q.z + q.w);
 }
 
-// Sum of two per-thread values over the warpgroup: one barrier.
+// Sum of two per-thread values over the warpgroup: one barrier. Within a warp
+// the first shuffle level splits the work (lanes 0-15 keep summing a, lanes
+// 16-31 b), so two sums cost five shuffles instead of ten.
 __device__ __forceinline__ float2 group_sum2(float a, float b, float *red, int &slot,
                                              const Bar &B) {
-  a = warp_sum(a);
-  b = warp_sum(b);
+  const int lane = B.tid & 31;
+  const bool hi = lane & 16;
+  float x = hi ? b : a;
+  x += __shfl_xor_sync(0xffffffffu, hi ? a : b, 16);
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   float *r = red + slot * 16;
-  if ((B.tid & 31) == 0) reinterpret_cast<float2 *>(r)[B.tid >> 5] = make_float2(a, b);
+  if ((lane & 15) == 0) r[(B.tid >> 5) * 2 + (lane >> 4)] = x;
   B.sync();
   float2 t = make_float2(0.f, 0.f);
 #pragma unroll
@@ -542,14 +548,21 @@ __device__ __forceinline__ float2 group_sum2(float a, float b, float *red, int &
   return t;
 }
 
-// Sum of up to four per-thread values over the warpgroup: one barrier.
+// Sum of four per-thread values over the warpgroup: one barrier. The first two
+// shuffle levels split the four sums over lane quarters (six shuffles, not 20).
 __device__ __forceinline__ float4 group_sum4(float4 v, float *red, int &slot, const Bar &B) {
-  v.x = warp_sum(v.x);
-  v.y = warp_sum(v.y);
-  v.z = warp_sum(v.z);
-  v.w = warp_sum(v.w);
+  const int lane = B.tid & 31;
+  const bool h16 = lane & 16, h8 = lane & 8;
+  float x0 = h16 ? v.z : v.x, x1 = h16 ? v.w : v.y;
+  x0 += __shfl_xor_sync(0xffffffffu, h16 ? v.x : v.z, 16);
+  x1 += __shfl_xor_sync(0xffffffffu, h16 ? v.y : v.w, 16);
+  float x = h8 ? x1 : x0;
+  x += __shfl_xor_sync(0xffffffffu, h8 ? x0 : x1, 8);
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  // lane 0: v.x, lane 8: v.y, lane 16: v.z, lane 24: v.w
   float *r = red + slot * 16;
-  if ((B.tid & 31) == 0) reinterpret_cast<float4 *>(r)[B.tid >> 5] = v;
+  if ((lane & 7) == 0) r[(B.tid >> 5) * 4 + (lane >> 3)] = x;
   B.sync();
   float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
