@@ -112,6 +112,9 @@ _sig(lib.als_rmse_work_bytes, c_sz)
 _sig(lib.als_rmse, c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_i32, c_i32, c_vp, c_vp,
      c_sz, c_vp)
 _sig(lib.als_predict, c_i32, c_i64, c_vp, c_vp, c_vp, c_i32, c_vp, c_i32, c_i32, c_vp, c_vp)
+_sig(lib.als_topk, c_i32, c_i64, c_vp, c_vp, c_i32, c_vp, c_i32, c_i64, c_i32, c_i32, c_vp, c_vp,
+     c_vp, c_vp, c_vp)
+_sig(lib.als_csr_to_csc, c_i32, c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp)
 _sig(lib.als_train, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i32, c_i64, c_f32,
      c_i32, c_vp, c_vp, c_vp, c_vp)
 _sig(lib.doALSWithCSR, None, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int,
@@ -486,6 +489,34 @@ def half_step(row_ptr, col, val, src, dst, lam: float, opts: Options | None = No
                              src.stride(0), _ptr(dst), dst.stride(0), lam,
                              ctypes.byref(opts or options()), _ptr(work), work.numel(),
                              _stream_handle(stream)))
+
+
+def topk(users, x, theta, k: int, seen_ptr=None, seen_col=None, stream=None):
+    """Top-k items per user (device tensors): returns (items int32 [nq, k],
+    scores float32 [nq, k]), leaving out the items in each user's row of the
+    (seen_ptr, seen_col) CSR when given."""
+    import torch
+    nq = users.shape[0]
+    n, f = theta.shape
+    items = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    scores = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    _check(lib.als_topk(nq, _ptr(users), _ptr(x), x.stride(0), _ptr(theta), theta.stride(0), n, f,
+                        k, _ptr(seen_ptr) if seen_ptr is not None else None,
+                        _ptr(seen_col) if seen_col is not None else None, _ptr(items),
+                        _ptr(scores), _stream_handle(stream)))
+    return items, scores
+
+
+def csr_to_csc(m: int, n: int, ptr, col, val, stream=None):
+    """Device CSR (int64 pointers) -> device CSC (col_ptr int64, rows int32, vals)."""
+    import torch
+    nnz = col.shape[0]
+    cptr = torch.empty(n + 1, dtype=torch.int64, device="cuda")
+    rows = torch.empty(max(nnz, 1), dtype=torch.int32, device="cuda")
+    vals = torch.empty(max(nnz, 1), dtype=torch.float32, device="cuda")
+    _check(lib.als_csr_to_csc(m, n, nnz, _ptr(ptr), _ptr(col), _ptr(val), _ptr(cptr), _ptr(rows),
+                              _ptr(vals), _stream_handle(stream)))
+    return cptr, rows[:nnz], vals[:nnz]
 
 
 def rmse(u, i, r, x, theta, stream=None) -> float:

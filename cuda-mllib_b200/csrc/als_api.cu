@@ -643,6 +643,27 @@ int als_predict(int64_t nt, const int32_t *u, const int32_t *i, const float *x, 
   return ALS_OK;
 }
 
+int als_topk(int64_t nq, const int32_t *users, const float *x, int32_t ldx, const float *t,
+             int32_t ldt, int64_t n, int32_t f, int32_t k, const int64_t *seen_ptr,
+             const int32_t *seen_col, int32_t *items, float *scores, cudaStream_t st) {
+  if (nq < 0 || n < 0 || f < 1 || f > 128 || k < 1 || k > 256 || ldx < f || ldt < f ||
+      n > INT32_MAX - 1 || (nq > 0 && (!users || !x || !t || !items || !scores)) ||
+      ((seen_ptr == nullptr) != (seen_col == nullptr)))
+    return fail(ALS_ERR_INVALID, "als_topk: bad args (1 <= k <= 256, 1 <= f <= 128)");
+  ALS_TRY(launch_topk(nq, users, x, ldx, t, ldt, n, f, k, seen_ptr, seen_col, items, scores, st),
+          "als_topk");
+  return ALS_OK;
+}
+
+int als_csr_to_csc(int64_t m, int64_t n, int64_t nnz, const int64_t *ptr, const int32_t *col,
+                   const float *val, int64_t *cptr, int32_t *crow, float *cval, cudaStream_t st) {
+  if (m < 0 || n < 0 || nnz < 0 || m > INT32_MAX || n > INT32_MAX || !ptr || !cptr ||
+      (nnz > 0 && (!col || !val || !crow || !cval)))
+    return fail(ALS_ERR_INVALID, "als_csr_to_csc: bad args");
+  ALS_TRY(csr_to_csc(m, n, nnz, ptr, col, val, cptr, crow, cval, st), "als_csr_to_csc");
+  return ALS_OK;
+}
+
 int als_train(const int64_t *csr_ptr, const int32_t *csr_col, const float *csr_val,
               const int64_t *csc_ptr, const int32_t *csc_row, const float *csc_val, int64_t m,
               int64_t n, int32_t f, int64_t nnz, float lambda, int32_t iterations,

@@ -1,6 +1,8 @@
 // Auxiliary kernels: degree-binned row ordering, pointer widening, factor
-// down-conversion, and the fused RMSE / predict gather.
+// down-conversion, the fused RMSE / predict gather, and top-k recommendation.
 #include <algorithm>
+#include <climits>
+#include <cmath>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -177,6 +179,106 @@ cudaError_t launch_predict(int64_t nt, const int32_t *u, const int32_t *i, const
                            const float *T, int ldt, int f, float *out, cudaStream_t st) {
   if (nt <= 0) return cudaSuccess;
   predict_kernel<<<kRmseBlocks, kRmseThreads, 0, st>>>(nt, u, i, X, ldx, T, ldt, f, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// top-k recommendation: for each query user, the k items of largest x_u . theta_i,
+// leaving out the items the user has already rated (its row of the training
+// CSR, columns ascending). One block per query: a tile of 256 item scores at a
+// time joins the running top list in shared memory through a bitonic sort of
+// 512 (score descending, item ascending) pairs; tiles with no score above the
+// current k-th are skipped after one block vote.
+// ---------------------------------------------------------------------------
+constexpr int kTopThreads = 256;
+
+__device__ __forceinline__ bool top_before(float sa, int ia, float sb, int ib) {
+  return sa > sb || (sa == sb && ia < ib);
+}
+
+__device__ __forceinline__ bool seen_by(const int32_t *cols, int64_t s, int64_t e, int item) {
+  while (s < e) {  // binary search in the ascending columns [s, e)
+    const int64_t mid = (s + e) >> 1;
+    const int c = cols[mid];
+    if (c == item) return true;
+    if (c < item) s = mid + 1;
+    else e = mid;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kTopThreads) topk_kernel(
+    int64_t nq, const int32_t *users, const float *X, int ldx, const float *T, int ldt, int64_t n,
+    int f, int k, const int64_t *seen_ptr, const int32_t *seen_col, int32_t *out_items,
+    float *out_scores) {
+  __shared__ float xs[128];
+  __shared__ float sc[2 * kTopThreads];
+  __shared__ int id[2 * kTopThreads];
+  const int t = threadIdx.x;
+  for (int64_t q = blockIdx.x; q < nq; q += gridDim.x) {
+    const int64_t u = users[q];
+    if (t < f) xs[t] = X[u * ldx + t];
+    sc[t] = sc[t + kTopThreads] = -INFINITY;
+    id[t] = id[t + kTopThreads] = INT_MAX;
+    const int64_t s0 = seen_ptr ? seen_ptr[u] : 0, s1 = seen_ptr ? seen_ptr[u + 1] : 0;
+    __syncthreads();
+    float kth = -INFINITY;
+    int kid = INT_MAX;
+    for (int64_t base = 0; base < n; base += kTopThreads) {
+      const int64_t i = base + t;
+      float s = -INFINITY;
+      int ii = INT_MAX;
+      if (i < n && !seen_by(seen_col, s0, s1, (int)i)) {
+        const float *th = T + i * ldt;
+        float a0 = 0.f, a1 = 0.f;
+        int c = 0;
+        for (; c + 1 < f; c += 2) {
+          a0 = fmaf(xs[c], th[c], a0);
+          a1 = fmaf(xs[c + 1], th[c + 1], a1);
+        }
+        if (c < f) a0 = fmaf(xs[c], th[c], a0);
+        s = a0 + a1;
+        ii = (int)i;
+      }
+      if (!__syncthreads_or(ii != INT_MAX && top_before(s, ii, kth, kid))) continue;
+      sc[kTopThreads + t] = s;
+      id[kTopThreads + t] = ii;
+      // bitonic sort of the 512 pairs, best first
+      for (int size = 2; size <= 2 * kTopThreads; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          __syncthreads();
+          const int a = 2 * t - (t & (stride - 1)), b = a + stride;
+          const bool best_first = (a & size) == 0;
+          const float sa = sc[a], sb = sc[b];
+          const int ia = id[a], ib = id[b];
+          if (top_before(sb, ib, sa, ia) == best_first) {
+            sc[a] = sb; sc[b] = sa;
+            id[a] = ib; id[b] = ia;
+          }
+        }
+      }
+      __syncthreads();
+      kth = sc[k - 1];
+      kid = id[k - 1];
+      __syncthreads();
+    }
+    for (int j = t; j < k; j += kTopThreads) {
+      out_items[q * k + j] = id[j] == INT_MAX ? -1 : id[j];
+      out_scores[q * k + j] = id[j] == INT_MAX ? -INFINITY : sc[j];
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_topk(int64_t nq, const int32_t *users, const float *X, int ldx, const float *T,
+                        int ldt, int64_t n, int f, int k, const int64_t *seen_ptr,
+                        const int32_t *seen_col, int32_t *out_items, float *out_scores,
+                        cudaStream_t st) {
+  if (nq <= 0) return cudaSuccess;
+  if (f < 1 || f > 128 || k < 1 || k > kTopThreads || n > INT32_MAX - 1) return cudaErrorInvalidValue;
+  const unsigned grid = (unsigned)std::min<int64_t>(nq, (int64_t)device_sm_count() * 8);
+  topk_kernel<<<grid, kTopThreads, 0, st>>>(nq, users, X, ldx, T, ldt, n, f, k, seen_ptr, seen_col,
+                                            out_items, out_scores);
   return cudaGetLastError();
 }
 

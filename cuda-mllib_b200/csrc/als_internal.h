@@ -99,6 +99,20 @@ cudaError_t launch_predict(int64_t nt, const int32_t *u, const int32_t *i, const
 
 int device_sm_count();
 
+// Top-k items per query user by x_u . theta_i, items of the user's training
+// row (seen_ptr/seen_col, may be null) left out; k <= 256, f <= 128.
+cudaError_t launch_topk(int64_t nq, const int32_t *users, const float *X, int ldx, const float *T,
+                        int ldt, int64_t n, int f, int k, const int64_t *seen_ptr,
+                        const int32_t *seen_col, int32_t *out_items, float *out_scores,
+                        cudaStream_t st);
+
+// CSR (m x n, nnz ratings) -> CSC on the device, rows ascending per column
+// (stable radix sort by column). Synchronises the stream; allocates its sort
+// scratch.
+cudaError_t csr_to_csc(int64_t m, int64_t n, int64_t nnz, const int64_t *ptr, const int32_t *col,
+                       const float *val, int64_t *cptr, int32_t *crow, float *cval,
+                       cudaStream_t st);
+
 // Learned CG warm start (als_mlp.cu). The net is opaque to callers.
 cudaError_t mlp_create(void **out, int f, int64_t cap, uint64_t seed, cudaStream_t st);
 void mlp_destroy(void *net);

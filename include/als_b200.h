@@ -208,6 +208,29 @@ int als_predict(int64_t nt, const int32_t *d_u, const int32_t *d_i, const float 
                 int32_t ldx, const float *d_theta, int32_t ldt, int32_t f, float *d_out,
                 cudaStream_t stream);
 
+/* Top-k recommendation (serving; no counterpart in the reference). For each of
+ * the nq users in d_users, the k items (k <= 256) of largest x_u . theta_i over
+ * all n items, best first (ties: lower item index), leaving out the items in
+ * the user's row of a CSR of already-rated items (d_seen_ptr / d_seen_col,
+ * columns ascending per row; both null to keep every item). Outputs are
+ * nq x k, row-major; an item of -1 (score -inf) pads users with fewer than k
+ * candidate items. f <= 128. */
+int als_topk(int64_t nq, const int32_t *d_users, const float *d_x, int32_t ldx,
+             const float *d_theta, int32_t ldt, int64_t n, int32_t f, int32_t k,
+             const int64_t *d_seen_ptr, const int32_t *d_seen_col, int32_t *d_items,
+             float *d_scores, cudaStream_t stream);
+
+/* CSR (m x n, nnz ratings; int64 row pointers) -> CSC, i.e. the CSR of the
+ * transpose (n x m), on the device: rows stay ascending within each column, so
+ * the result equals als_csr_transpose's. A caller that keeps only one
+ * orientation of the rating matrix can build the other for als_model_create.
+ * Allocates its sort scratch and synchronises the stream. No counterpart in
+ * the reference, whose loadCSRSparseMatrixBin (als.cu:914-933) gives a CSR
+ * only. */
+int als_csr_to_csc(int64_t m, int64_t n, int64_t nnz, const int64_t *d_row_ptr,
+                   const int32_t *d_col, const float *d_val, int64_t *d_col_ptr,
+                   int32_t *d_row, float *d_val_t, cudaStream_t stream);
+
 /* Learned warm start: the MLP that maps a row's features
  * [b_u / n_u, diag(A_u) / n_u, log1p(n_u) / 8] (2f+1 values, BF16, row stride
  * als_mlp_feature_stride) to x0 (f floats). Layers 2f+1 -> 256 -> 256 -> f with
