@@ -583,9 +583,11 @@ def get_dropin_options() -> Options:
 
 
 def do_als_with_csr(row_ptr32: np.ndarray, col: np.ndarray, val: np.ndarray, theta: np.ndarray,
-                    m: int, n: int, f: int, lam: float, x_batch: int = 1) -> np.ndarray:
+                    m: int, n: int, f: int, lam: float, x_batch: int = 1,
+                    out: np.ndarray | None = None) -> np.ndarray:
     """Run the drop-in ``doALSWithCSR``: CSR into mallocBest memory (freed by the
-    callee), theta and X in host memory; returns X (m x f)."""
+    callee), theta and X in host memory; returns X (m x f), written into ``out``
+    (C-contiguous float32, pageable or pinned) when it is given."""
     rt = _rt()
     nnz = len(col)
     ptrs = []
@@ -598,6 +600,11 @@ def do_als_with_csr(row_ptr32: np.ndarray, col: np.ndarray, val: np.ndarray, the
             raise AlsError(ALS_ERR_CUDA, "cudaMemcpy failed")
         ptrs.append(p)
     th = np.ascontiguousarray(theta, np.float32)
-    X = np.zeros((m, f), np.float32)
+    if out is None:
+        X = np.zeros((m, f), np.float32)
+    else:
+        if out.dtype != np.float32 or out.shape != (m, f) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of shape (m, f)")
+        X = out
     lib.doALSWithCSR(None, ptrs[0], ptrs[1], ptrs[2], _ptr(th), _ptr(X), m, n, f, nnz, lam, x_batch)
     return X

@@ -38,6 +38,8 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -1008,6 +1010,37 @@ cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
 // ---------------------------------------------------------------------------
 // host planning of the work list
 // ---------------------------------------------------------------------------
+namespace {
+// Host memory of the planner (the row pointers read back and the item list
+// before its upload), kept across calls: a fresh allocation costs one page
+// fault per 4 KB on first touch, which at the Netflix shape (19 MB) took
+// longer than the planning itself. Pinned when the driver grants it, so the
+// upload is one DMA. Guarded by plan_host_mu; every plan_ws call synchronises
+// its stream before it lets go, so no copy from it is in flight then.
+std::mutex plan_host_mu;
+char *plan_host = nullptr;
+size_t plan_host_cap = 0;
+bool plan_host_pinned = false;
+
+char *plan_host_buffer(size_t bytes) {
+  if (bytes <= plan_host_cap) return plan_host;
+  if (plan_host) {
+    if (plan_host_pinned) cudaFreeHost(plan_host);
+    else std::free(plan_host);
+  }
+  plan_host_cap = 0;
+  const size_t want = bytes + bytes / 4;
+  plan_host_pinned = cudaHostAlloc((void **)&plan_host, want, cudaHostAllocPortable) == cudaSuccess;
+  if (!plan_host_pinned) {
+    cudaGetLastError();
+    plan_host = static_cast<char *>(std::malloc(want));
+    if (!plan_host) return nullptr;
+  }
+  plan_host_cap = want;
+  return plan_host;
+}
+}  // namespace
+
 cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int grid, int np,
                     int src_rows, WsPlan *plan, void **mem, cudaStream_t st) {
   *mem = nullptr;
@@ -1015,98 +1048,104 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
   plan->src_rows = src_rows;
   plan->part_ld = np + 4;
   if (count <= 0) return cudaSuccess;
-  std::vector<int64_t> ptr((size_t)count + 1);
-  cudaError_t e = cudaMemcpyAsync(ptr.data(), d_row_ptr + begin, sizeof(int64_t) * (count + 1),
+  std::lock_guard<std::mutex> lk(plan_host_mu);
+  // A row of d > split ratings becomes ceil(d / split) <= d / split + 1
+  // chunks and split >= nnz / (4 grid), so there are at most count + 4 grid
+  // items.
+  const size_t ptr_bytes = (sizeof(int64_t) * ((size_t)count + 1) + 255) / 256 * 256;
+  char *host = plan_host_buffer(ptr_bytes + sizeof(WorkItem) * ((size_t)count + 4 * (size_t)grid));
+  if (!host) return cudaErrorMemoryAllocation;
+  int64_t *ptr = reinterpret_cast<int64_t *>(host);
+  WorkItem *out = reinterpret_cast<WorkItem *>(host + ptr_bytes);
+  cudaError_t e = cudaMemcpyAsync(ptr, d_row_ptr + begin, sizeof(int64_t) * (count + 1),
                                   cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return e;
   const int64_t nnz = ptr[(size_t)count] - ptr[0];
   // rows longer than a quarter of a CTA's fair share are split
   const int64_t split = std::max<int64_t>(8192, (nnz + 4LL * grid - 1) / (4LL * grid));
-  std::vector<WorkItem> items;
-  items.reserve((size_t)count + 64);
+  // Order: largest item first, ties in row order (a stable counting sort on
+  // the item size, at most `split` ratings), then dealt to CTAs round robin
+  // (CTA c takes sorted items c, c + grid, ...: balanced by the sort). Within
+  // a CTA the order zigzags between its largest and smallest items, so rows
+  // that load the producers (many ratings) alternate with rows that load the
+  // solvers (few ratings) instead of coming in two long runs. Both steps are
+  // a position per item: one pass counts, the second writes each item once
+  // to its final place.
+  std::vector<int64_t> start((size_t)split + 2, 0);
   std::vector<int> hn, hb;
   int slots = 0;
+  int64_t N = 0;
   for (int64_t r = 0; r < count; ++r) {
-    const int64_t s = ptr[(size_t)r], e2 = ptr[(size_t)r + 1], d = e2 - s;
-    const int u = (int)(begin + r);
+    const int64_t d = ptr[(size_t)r + 1] - ptr[(size_t)r];
     if (d > split) {
-      const int nch = (int)((d + split - 1) / split);
-      const int h = (int)hn.size();
-      hn.push_back(nch);
+      const int64_t nch = (d + split - 1) / split;
+      start[0] += nch - 1;  // full chunks
+      ++start[(size_t)(split - (d - (nch - 1) * split))];
+      hn.push_back((int)nch);
       hb.push_back(slots);
-      for (int ch = 0; ch < nch; ++ch) {
-        WorkItem w;
-        w.s = s + ch * split;
-        w.e = std::min<int64_t>(e2, s + (ch + 1) * split);
-        w.u = u;
-        w.deg = (int)d;
-        w.part = slots + ch;
-        w.heavy = h;
-        items.push_back(w);
-      }
-      slots += nch;
+      slots += (int)nch;
+      N += nch;
     } else {
-      WorkItem w;
-      w.s = s;
-      w.e = e2;
-      w.u = u;
-      w.deg = (int)d;
-      w.part = -1;
-      w.heavy = -1;
-      items.push_back(w);
+      ++start[(size_t)(split - d)];
+      ++N;
     }
   }
-  // largest first, ties in row order: a stable counting sort on the item size
-  // (at most `split` ratings), linear in the number of rows
   {
-    std::vector<int64_t> start((size_t)split + 2, 0);
-    for (const WorkItem &w : items) ++start[(size_t)(split - (w.e - w.s))];
     int64_t acc = 0;
     for (auto &v : start) {
       const int64_t c = v;
       v = acc;
       acc += c;
     }
-    std::vector<WorkItem> sorted(items.size());
-    for (const WorkItem &w : items) sorted[(size_t)start[(size_t)(split - (w.e - w.s))]++] = w;
-    items.swap(sorted);
   }
-  // CTA c takes items c, c + grid, c + 2 grid, ... (balanced by the sort).
-  // Within a CTA the order zigzags between its largest and smallest items,
-  // so rows that load the producers (many ratings) alternate with rows that
-  // load the solvers (few ratings) instead of coming in two long runs.
-  {
-    const int64_t N = (int64_t)items.size(), G = grid;
-    std::vector<WorkItem> zig(items.size());
-    for (int64_t c = 0; c < std::min<int64_t>(G, N); ++c) {
-      const int64_t nc = (N - c + G - 1) / G;
-      for (int64_t j = 0; j < nc; ++j) {
-        const int64_t k = (j & 1) ? nc - 1 - j / 2 : j / 2;
-        zig[(size_t)(c + j * G)] = items[(size_t)(c + k * G)];
+  const int64_t G = grid;
+  auto place = [&](const WorkItem &w) {
+    const int64_t k = start[(size_t)(split - (w.e - w.s))]++;  // rank, largest first
+    const int64_t c = k % G, q = k / G, nc = (N - c + G - 1) / G;
+    const int64_t j = q < (nc + 1) / 2 ? 2 * q : 2 * (nc - 1 - q) + 1;  // zigzag slot
+    out[(size_t)(c + j * G)] = w;
+  };
+  for (int64_t r = 0, h = 0; r < count; ++r) {
+    const int64_t s = ptr[(size_t)r], e2 = ptr[(size_t)r + 1], d = e2 - s;
+    WorkItem w;
+    w.u = (int)(begin + r);
+    w.deg = (int)d;
+    if (d > split) {
+      for (int ch = 0; ch < hn[(size_t)h]; ++ch) {
+        w.s = s + ch * split;
+        w.e = std::min<int64_t>(e2, s + (ch + 1) * split);
+        w.part = hb[(size_t)h] + ch;
+        w.heavy = (int)h;
+        place(w);
       }
+      ++h;
+    } else {
+      w.s = s;
+      w.e = e2;
+      w.part = -1;
+      w.heavy = -1;
+      place(w);
     }
-    items.swap(zig);
   }
   const size_t nh = hn.size();
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-  const size_t oI = 0, oN = al(sizeof(WorkItem) * items.size()), oB = oN + al(4 * (nh + 1)),
+  const size_t oI = 0, oN = al(sizeof(WorkItem) * (size_t)N), oB = oN + al(4 * (nh + 1)),
                oC = oB + al(4 * (nh + 1)), oP = oC + al(4 * (nh + 1)),
                oK = oP + al(sizeof(float) * (size_t)slots * 128 * plan->part_ld + 16),
                total = oK + al(sizeof(float) * (size_t)grid * ws::kMaxGroups * kCholFloats);
   char *d = nullptr;
   if ((e = cudaMalloc(&d, total)) != cudaSuccess) return e;
-  e = cudaMemcpyAsync(d + oI, items.data(), sizeof(WorkItem) * items.size(),
-                      cudaMemcpyHostToDevice, st);
+  e = cudaMemcpyAsync(d + oI, out, sizeof(WorkItem) * (size_t)N, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && nh)
     e = cudaMemcpyAsync(d + oN, hn.data(), 4 * nh, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && nh)
     e = cudaMemcpyAsync(d + oB, hb.data(), 4 * nh, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d + oC, 0, 4 * (nh + 1), st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors go out of scope
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host memory is reused after this
   if (e != cudaSuccess) { cudaFree(d); return e; }
   plan->items = (const WorkItem *)(d + oI);
-  plan->nitems = (int)items.size();
+  plan->nitems = (int)N;
   plan->heavy_nchunks = (const int *)(d + oN);
   plan->heavy_base = (const int *)(d + oB);
   plan->heavy_count = (unsigned *)(d + oC);

@@ -105,6 +105,31 @@ def test_dropin_doALSWithCSR(ml_small, f):
     assert np.array_equal(X, X2)
 
 
+def test_dropin_staged_copies_match_pinned():
+    """theta and X above 32 MB in pageable host memory travel through the
+    drop-in's pinned staging (four host workers, two 8 MB halves each), in
+    five chunks with a partial last one, so one worker reuses its first half;
+    pinned host buffers are copied directly. Both give the same X,
+    bit for bit, for the user side (X staged on the way down) and the item side
+    (theta staged on the way up)."""
+    r = A.synth(A.scaled_config("netflix", 0.2), seed=4)
+    f, lam = 100, 0.05
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+    th = A.init_factors(r.n, f, 5)
+    ptr32, cptr32 = r.csr_ptr.astype(np.int32), r.csc_ptr.astype(np.int32)
+    X_pg = A.do_als_with_csr(ptr32, r.csr_col, r.csr_val, th, r.m, r.n, f, lam)
+    assert X_pg.nbytes > 32 << 20 and X_pg.nbytes % (16 << 20)
+    X_pin = A.do_als_with_csr(ptr32, r.csr_col, r.csr_val, pin(th), r.m, r.n, f, lam,
+                              out=pin(np.zeros((r.m, f), np.float32)))
+    assert np.isfinite(X_pg).all() and np.array_equal(X_pg, X_pin)
+    T_pg = A.do_als_with_csr(cptr32, r.csc_row, r.csc_val, X_pg, r.n, r.m, f, lam)
+    T_pin = A.do_als_with_csr(cptr32, r.csc_row, r.csc_val, pin(X_pg), r.n, r.m, f, lam,
+                              out=pin(np.zeros((r.n, f), np.float32)))
+    assert np.isfinite(T_pg).all() and np.array_equal(T_pg, T_pin)
+    X_ref, _ = O.half_step(r.csr_ptr[:2001], r.csr_col, r.csr_val, th, lam)
+    assert rel_rows(X_pg[:2000], X_ref).max() < TOL
+
+
 def test_rmse_and_predict(ml_small):
     r, f = ml_small, 16
     rng = np.random.default_rng(0)
