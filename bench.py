@@ -380,7 +380,7 @@ def run_engine(args):
         cptr32 = r.csc_ptr.astype(np.int32)
         pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
         host = [pin(a) for a in (ptr32, r.csr_col, r.csr_val, cptr32, r.csc_row, r.csc_val)]
-        e2e_steps = max(1, min(args.steps, 3))
+        e2e_steps = max(1, min(args.steps, 5))
         torch.cuda.synchronize(dev)
         times = []
         for _ in range(e2e_steps + 1):
