@@ -41,11 +41,14 @@ def parse():
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--config", default="netflix")
     p.add_argument("--scale", type=float, default=1.0, help="shrink m, n (nnz by scale^2)")
+    p.add_argument("--row-scale", type=float, default=1.0, help="shrink m and nnz, keep n")
     p.add_argument("--precision", default="bf16", choices=["fp32", "bf16", "fp16"])
     p.add_argument("--solver", default="cg", choices=["cholesky", "cg"])
     p.add_argument("--warm", default="previous", choices=["zero", "previous", "mlp"],
                    help="CG starting point")
     p.add_argument("--jacobi", action="store_true", help="diagonal-preconditioned CG")
+    p.add_argument("--graph", action="store_true",
+                   help="time the iteration as one CUDA graph replay (users + items launches)")
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -55,7 +58,17 @@ def parse():
 
 def cfg_of(args):
     import als_b200 as A
+    if args.row_scale != 1.0:
+        return A.row_scaled_config(args.config, args.row_scale)
     return A.scaled_config(args.config, args.scale) if args.scale != 1.0 else dict(A.CONFIGS[args.config])
+
+
+def workload_name(args):
+    if args.config == "netflix" and args.scale == 1.0 and args.row_scale == 1.0:
+        return WORKLOAD
+    if args.row_scale != 1.0:
+        return f"{args.config} rows x{args.row_scale}"
+    return f"{args.config} x{args.scale}" if args.scale != 1.0 else args.config
 
 
 def peaks():
@@ -219,7 +232,7 @@ def run_reference(args):
             "ms_per_step": round(full / (gflops * 1e9) * 1e3, 3),
             "sec_per_iter": round(full / (gflops * 1e9), 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": WORKLOAD if args.scale == 1.0 else f"{args.config} x{args.scale}",
+            "config": {"workload": workload_name(args),
                        "f": f, "lambda": lam, "m": r.m, "n": r.n, "nnz_train": r.nnz},
             "cpu_baseline": {"value": round(gflops, 3), "unit": "GFLOP/s", "cores": cores,
                              "kind": "port", "sample": sample},
@@ -250,7 +263,8 @@ def run_engine(args):
     solver = {"cholesky": A.SOLVER_CHOLESKY, "cg": A.SOLVER_CG}[args.solver]
     warm = {"zero": A.WARM_ZERO, "previous": A.WARM_PREVIOUS, "mlp": A.WARM_MLP}[args.warm]
     opts = A.options(precision=prec, solver=solver, warm_start=warm,
-                     cg_jacobi=1 if args.jacobi else 0)
+                     cg_jacobi=1 if args.jacobi else 0, use_graph=1 if args.graph else 0)
+    graph = args.graph and args.warm != "mlp" and world == 1
     stream = torch.cuda.Stream(device=dev)
     th0 = A.init_factors(r.n, f, args.seed + 100)
     with torch.cuda.stream(stream):
@@ -265,6 +279,11 @@ def run_engine(args):
         # one launch of the fused rows kernel per half-step
         if ev is not None:
             ev[0].record(stream)
+        if graph and ev is not None:
+            model.iterate(lam, 1)  # replay of the captured users + items launches
+            ev[1].record(stream)
+            ev[2].record(stream)
+            return
         model.half_step(A.SIDE_USERS, lam)
         if shard:
             shard.gather(A.SIDE_USERS)
@@ -278,6 +297,8 @@ def run_engine(args):
 
     for _ in range(args.warmup):
         iteration()
+    if graph:
+        model.iterate(lam, 1)  # capture (after the warm-up has tuned both sides) and replay once
     torch.cuda.synchronize(dev)
     model.stats(reset=True)
     if world > 1:
@@ -293,6 +314,9 @@ def run_engine(args):
         dist.barrier()
     users_ms = np.array([e[0].elapsed_time(e[1]) for e in evs])
     items_ms = np.array([e[1].elapsed_time(e[2]) for e in evs])
+    if graph:
+        # one graph replay per step: the two launches are not timed apart
+        users_ms = items_ms = (users_ms + items_ms) / 2
     print("per-step users ms", np.round(users_ms, 2).tolist(), "items ms",
           np.round(items_ms, 2).tolist(), file=sys.stderr)
     step_ms = users_ms + items_ms
@@ -339,8 +363,9 @@ def run_engine(args):
             "peak_kind": f"{src} HBM copy bandwidth",
             "kernel": "rows kernel (gather + hermitian + solve), mean of the two launches per step",
             "bytes_per_launch": round(avg_bytes), "bytes_formula": "nnz*(8+f*s) + rows*(8+8f+f*s)",
-            "items_launch": {"ms": round(float(items_ms.mean()), 3), "achieved": round(items_gbs, 1),
-                             "frac": round(items_gbs / hbm, 4)},
+            "items_launch": None if graph else {"ms": round(float(items_ms.mean()), 3),
+                                                "achieved": round(items_gbs, 1),
+                                                "frac": round(items_gbs / hbm, 4)},
             "tensor": {"syrk_flops_per_launch": r.nnz * f * (f + 1), "achieved_tflops": round(syrk_tflops, 2),
                        "peak": tf_sust, "frac": round(syrk_tflops / tf_sust, 4),
                        "peak_kind": f"{src} bf16 dense sustained"},
@@ -354,11 +379,12 @@ def run_engine(args):
                 "sec_per_iter": round(med_ms / 1e3, 5), "higher_is_better": True,
                 "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
                 "dtype": args.precision, "data": "synthetic",
-                "config": {"workload": WORKLOAD if args.scale == 1.0 else f"{args.config} x{args.scale}",
+                "config": {"workload": workload_name(args),
                            "f": f, "lambda": lam, "m": r.m, "n": r.n, "nnz_train": r.nnz,
                            "n_test": int(len(r.test_r)), "precision": args.precision,
                            "solver": args.solver, "warm_start": args.warm,
                            "cg_jacobi": args.jacobi, "seed": args.seed,
+                           "cuda_graph": bool(graph),
                            "l2": "inputs larger than L2 (CSR+CSC %.2f GB per iteration)" % (
                                (r.nnz * 16 + (r.m + r.n) * 8) / 1e9),
                            "parallelism": f"rows sharded x{world}" if world > 1 else "1 GPU",

@@ -225,6 +225,13 @@ CONFIGS = {
                   iters=10),
 }
 CONFIGS["netflix128"] = dict(CONFIGS["netflix"], f=128)
+# Tall-skinny shape with ~3.1 billion ratings (int64 row pointers): lognormal
+# users (mean ~62), Zipf s=1.05 items, float ratings in [0, 5]; 1% held out
+CONFIGS["hugewiki"] = dict(m=50_082_604, n=39_781, target_nnz=3_100_000_000, planted_rank=100,
+                           factor_sigma=100 ** -0.25, noise_sigma=0.5, mu=2.5, rating_min=0,
+                           rating_max=5, integer_ratings=0, degree_law=0, degree_p1=1.2,
+                           degree_min=1, degree_max=0, item_zipf_s=1.05, test_fraction=0.01,
+                           f=100, lam=0.05, iters=10)
 
 
 def scaled_config(name: str, scale: float) -> dict:
@@ -235,6 +242,14 @@ def scaled_config(name: str, scale: float) -> dict:
     c["target_nnz"] = max(16, int(c["target_nnz"] * scale * scale))
     if c["degree_max"]:
         c["degree_max"] = max(1, int(c["degree_max"] * scale))
+    return c
+
+
+def row_scaled_config(name: str, scale: float) -> dict:
+    """A configuration with m and nnz scaled (n and the degree laws kept)."""
+    c = dict(CONFIGS[name])
+    c["m"] = max(8, int(c["m"] * scale))
+    c["target_nnz"] = max(16, int(c["target_nnz"] * scale))
     return c
 
 
@@ -341,6 +356,30 @@ class Model:
         if theta0 is None:
             theta0 = init_factors(self.n, f, seed)
         self.set_theta(torch.from_numpy(np.ascontiguousarray(theta0, np.float32)).to(dev))
+
+    @classmethod
+    def from_device(cls, m: int, n: int, f: int, nnz: int, arrays, test, opts=None,
+                    stream=None, theta0: np.ndarray | None = None, seed: int = 2):
+        """A model over rating arrays already on the device: ``arrays`` is
+        (csr_ptr, csr_col, csr_val, csc_ptr, csc_row, csc_val) as CUDA tensors
+        (int64 pointers, which may start at any offset into col/val), ``test``
+        is (u, i, r). The tensors stay borrowed for the model's lifetime."""
+        import torch
+        self = cls.__new__(cls)
+        self.torch = torch
+        self.m, self.n, self.f = m, n, f
+        self._dev = list(arrays)
+        self.test = list(test)
+        self.opts = opts or options()
+        self.stream = _stream_handle(stream)
+        h = c_vp()
+        _check(lib.als_model_create(ctypes.byref(h), m, n, f, nnz, *[_ptr(x) for x in self._dev],
+                                    ctypes.byref(self.opts), self.stream))
+        self.handle = h
+        if theta0 is None:
+            theta0 = init_factors(n, f, seed)
+        self.set_theta(torch.from_numpy(np.ascontiguousarray(theta0, np.float32)).cuda())
+        return self
 
     def close(self):
         if getattr(self, "handle", None):
