@@ -191,6 +191,25 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g, int np, uint
 }
 
 cudaError_t gemm(const GemmArgs &g, cudaStream_t st) {
+  if (g.N > 256 && g.M > 0 && g.K > 0 && g.N % 8 == 0) {
+    // One accumulator holds at most 256 columns: split N into near-equal
+    // blocks of a multiple of 8 columns (the first-layer weight gradient at
+    // f = 128 has N = 264) and run one GEMM per block.
+    const int nb = (g.N + 255) / 256, w = ((g.N + nb - 1) / nb + 7) / 8 * 8;
+    for (int n0 = 0; n0 < g.N; n0 += w) {
+      GemmArgs h = g;
+      h.N = std::min(w, g.N - n0);
+      h.B = g.b_mn ? g.B + n0 : g.B + (int64_t)n0 * g.ldb;
+      if (g.bias) h.bias = g.bias + n0;
+      if (g.aux) h.aux = g.aux + n0;
+      if (g.C32) h.C32 = g.C32 + n0;
+      if (g.C16) h.C16 = g.C16 + n0;
+      if (g.Z) h.Z = g.Z + n0;
+      const cudaError_t e = gemm(h, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
   if (g.N <= 0 || g.N > 256 || g.M <= 0 || g.K <= 0) return cudaErrorInvalidValue;
   if (g.K % 8 || g.lda % 8 || g.ldb % 8) return cudaErrorInvalidValue;
   if ((g.a_mn && g.M % 8) || (g.b_mn && g.N % 8)) return cudaErrorInvalidValue;

@@ -129,7 +129,7 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
   unsigned uses0 = 0, uses1 = 0;  // commits issued per stage buffer
   unsigned acc_phase = 0;
   int rslot = 0;
-  unsigned long long n_rows = 0, n_ref = 0, n_bad = 0, n_steps = 0, n_fb = 0;
+  unsigned long long n_rows = 0, n_ref = 0, n_bad = 0, n_steps = 0, n_fb = 0, n_r0 = 0;
   const uint32_t lbo = (tc::KS / 8) * 1024, sbo = 1024;
   const uint32_t stage0 = tc::smem_u32(base);
   const int rchunk = f >> 3, rpos = f & 7;
@@ -237,11 +237,22 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
         q = fmaf(arow[k + 2], p4.z, q);
         q = fmaf(arow[k + 3], p4.w, q);
       }
+      if (sv.x0) {
+        // Scale the warm start along its own direction: alpha = x0.b / x0.A x0
+        // minimises the A-norm error of alpha * x0, so no start is worse than zero.
+        const float xb = cta_sum<NT>(x * bm, red, rslot);
+        const float xq = cta_sum<NT>(x * q, red, rslot);
+        float sc = xb / xq;
+        if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
+        x *= sc;
+        q *= sc;
+      }
       float r = live ? bm - q : 0.f;
       float p = r;
       float rr = cta_sum<NT>(r * r, red, rslot);
       const float bb = cta_sum<NT>(bm * bm, red, rslot);
       const float target = sv.cg_tol2 * bb;
+      if (tid == 0 && bb > 0.f) n_r0 += (unsigned long long)(1e6f * sqrtf(rr / bb));
       int it = 0;
       bool conv = rr <= target;
       while (!conv && it < sv.cg_max_steps) {
@@ -337,6 +348,7 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
     if (n_bad) atomicAdd(&a.counters->not_spd, n_bad);
     if (n_steps) atomicAdd(&a.counters->cg_steps, n_steps);
     if (n_fb) atomicAdd(&a.counters->cg_fallback, n_fb);
+    if (n_r0) atomicAdd(&a.counters->r0_micro, n_r0);
   }
   __syncthreads();
   if (misc[3]) {  // aborted: drain any MMA still in flight before freeing TMEM

@@ -30,7 +30,7 @@ def _batch(f, B, ldf, seed):
     return F[:, :2 * f + 1].astype(np.float64), T, Fd, torch.from_numpy(T).cuda()
 
 
-@pytest.mark.parametrize("f", [16, 100])
+@pytest.mark.parametrize("f", [16, 100, 128])
 def test_gradients_match_cpu_oracle(f):
     net = A.Mlp(f, capacity=256, seed=3)
     params = [p.astype(np.float64) for p in net.get_params()]
@@ -70,14 +70,17 @@ def test_training_reduces_loss():
     assert l1 < 0.1 * l0, (l0, l1)
 
 
-def test_learned_warm_start_gain_in_als():
+@pytest.mark.parametrize("f", [100, 128])
+def test_learned_warm_start_gain_in_als(f):
     """Iterations 1-3 train the net on the solved rows; in iterations 4-6 CG
     starts from the net's x0 (scaled optimally along its direction). Compared
     with starting from zero, the starting residual is far smaller; CG step
-    counts and the previous-iterate start are reported alongside."""
+    counts and the previous-iterate start are reported alongside. f = 128 is
+    the rank of the learned-warm-start workload (first-layer width 2f+1 = 257,
+    so its weight gradient spans two accumulator blocks)."""
     cfg = A.scaled_config("netflix", 0.05)
     r = A.synth(cfg, seed=9)
-    f, lam = 100, 0.05
+    lam = 0.05
     th0 = A.init_factors(r.n, f, 3)
     steps, rmse, r0 = {}, {}, {}
     for name, warm in (("zero", A.WARM_ZERO), ("previous", A.WARM_PREVIOUS), ("mlp", A.WARM_MLP)):
