@@ -32,6 +32,18 @@ namespace als {
 
 
 
+// v with its 16-bit element pos (0..7) replaced by bits, by selects (no
+// dynamic indexing, so v stays in registers)
+__device__ __forceinline__ uint4 patch16(uint4 v, int pos, uint16_t bits) {
+  const int sh = (pos & 1) * 16, w = pos >> 1;
+  const uint32_t keep = ~(0xFFFFu << sh), put = (uint32_t)bits << sh;
+  v.x = w == 0 ? (v.x & keep) | put : v.x;
+  v.y = w == 1 ? (v.y & keep) | put : v.y;
+  v.z = w == 2 ? (v.z & keep) | put : v.z;
+  v.w = w == 3 ? (v.w & keep) | put : v.w;
+  return v;
+}
+
 template <int FP>
 struct TcCfg {
   static constexpr int T8 = FP / 8;
@@ -84,6 +96,9 @@ __global__ void __launch_bounds__(TcCfg<FP>::NT)
 rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
   using C = TcCfg<FP>;
   constexpr int LDS = C::LDS, NT = C::NT;
+  // 16-byte pieces per thread and stage: a stage holds KS rows of at most
+  // (FP + 8) / 8 pieces (row stride roundup8(f + 1) <= FP + 8)
+  constexpr int kQ = (tc::KS * ((FP + 8) / 8) + NT - 1) / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // 1024-aligned base for the swizzled stages
   unsigned char *base = smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023);
@@ -164,16 +179,47 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
       const int krows = (kc + 15) & ~15;
       unsigned char *stg = base + (size_t)buf * g.stage_bytes;
       if (okw) {
-        for (int q = tid; q < krows * g.chunks; q += NT) {
+        // Each thread copies up to kQ 16-byte pieces of the stage. The column
+        // indices and ratings are read first and the factor pieces are then
+        // loaded back to back, so a thread waits on two memory latencies per
+        // stage instead of two per piece.
+        const int total = krows * g.chunks;
+        int64_t item[kQ];
+        float rv[kQ];
+#pragma unroll
+        for (int i = 0; i < kQ; ++i) {
+          const int q = tid + i * NT, k = q / g.chunks, j = q - k * g.chunks;
+          const bool in = q < total && k < kc;
+          item[i] = in ? (int64_t)a.col[k0 + k] : 0;
+          rv[i] = (in && j == rchunk) ? a.val[k0 + k] : 0.f;
+        }
+        uint4 v[kQ];
+#pragma unroll
+        for (int i = 0; i < kQ; ++i) {
+          const int q = tid + i * NT, k = q / g.chunks, j = q - k * g.chunks;
+          v[i] = make_uint4(0, 0, 0, 0);
+          if (q < total && k < kc) v[i] = __ldg(reinterpret_cast<const uint4 *>(src + item[i] * a.ld_src) + j);
+        }
+#pragma unroll
+        for (int i = 0; i < kQ; ++i) {
+          const int q = tid + i * NT, k = q / g.chunks, j = q - k * g.chunks;
+          if (q < total) {
+            if (k < kc && j == rchunk) v[i] = patch16(v[i], rpos, tc::to_bits<LP>(rv[i]));
+            const int atom = j >> 3, c = j & 7, kg = k >> 3, kr = k & 7;
+            *reinterpret_cast<uint4 *>(stg + atom * lbo + kg * 1024 + kr * 128 + ((c ^ kr) << 4)) = v[i];
+          }
+        }
+        // pieces beyond kQ per thread (none while ld <= FP + 8): one at a time
+        for (int q = tid + kQ * NT; q < total; q += NT) {
           const int k = q / g.chunks, j = q - k * g.chunks;
-          uint4 v = make_uint4(0, 0, 0, 0);
+          uint4 w = make_uint4(0, 0, 0, 0);
           if (k < kc) {
-            const int64_t item = a.col[k0 + k];
-            v = __ldg(reinterpret_cast<const uint4 *>(src + item * a.ld_src) + j);
-            if (j == rchunk) reinterpret_cast<uint16_t *>(&v)[rpos] = tc::to_bits<LP>(a.val[k0 + k]);
+            const int64_t it = a.col[k0 + k];
+            w = __ldg(reinterpret_cast<const uint4 *>(src + it * a.ld_src) + j);
+            if (j == rchunk) reinterpret_cast<uint16_t *>(&w)[rpos] = tc::to_bits<LP>(a.val[k0 + k]);
           }
           const int atom = j >> 3, c = j & 7, kg = k >> 3, kr = k & 7;
-          *reinterpret_cast<uint4 *>(stg + atom * lbo + kg * 1024 + kr * 128 + ((c ^ kr) << 4)) = v;
+          *reinterpret_cast<uint4 *>(stg + atom * lbo + kg * 1024 + kr * 128 + ((c ^ kr) << 4)) = w;
         }
       }
       tc::fence_proxy_async();

@@ -85,6 +85,23 @@ def test_powerlaw_degrees():
     assert r.csr_val.min() >= 0 and r.csr_val.max() <= 100
 
 
+def test_tall_skinny_row_scaled():
+    """The 3.1-billion-rating tall-skinny shape with a thousandth of its users:
+    all 39,781 items kept, mean user degree ~62, float ratings in [0, 5], 1%
+    held out, and the row and item sums of the two orientations agree."""
+    c = A.row_scaled_config("hugewiki", 0.001)
+    assert c["n"] == A.CONFIGS["hugewiki"]["n"] and c["m"] == 50_082
+    r = A.synth(c, seed=3)
+    assert r.n == 39_781 and r.m == 50_082
+    total = r.nnz + len(r.test_r)
+    assert 55 < total / r.m < 70
+    assert 0.007 < len(r.test_r) / total < 0.013
+    assert r.csr_val.min() >= 0.0 and r.csr_val.max() <= 5.0
+    assert not np.all(r.csr_val == np.round(r.csr_val))  # float ratings
+    assert r.csc_ptr[-1] == r.nnz
+    assert np.array_equal(np.bincount(r.csc_row, minlength=r.m), np.diff(r.csr_ptr))
+
+
 def test_init_factors_seeded():
     a = A.init_factors(100, 10, 3)
     b = A.init_factors(100, 10, 3, threads=2)
