@@ -25,6 +25,9 @@ struct Fp32Cfg {
   static constexpr int NTILES = T8 * (T8 + 1) / 2;
   static constexpr int NT = ((NTILES + 31) / 32) * 32;
   static constexpr int KC = 32;       // items staged per chunk
+  // CTAs per SM the register allocation must allow (at most ~168 registers a
+  // thread), so the staged loads do not cost occupancy
+  static constexpr int kMinBlocks = 65536 / (NT * 168) > 0 ? 65536 / (NT * 168) : 1;
   static constexpr int LDS = FP + 1;  // row stride of S (odd: conflict-free columns)
   static constexpr size_t kStage = (size_t)KC * FP * 4 + (size_t)KC * 8;
   static constexpr size_t kS = (size_t)FP * LDS * 4;
@@ -39,7 +42,7 @@ __device__ __forceinline__ void store_lp(void *p, int64_t idx, float v) {
 }
 
 template <int FP, bool VEC>
-__global__ void __launch_bounds__(Fp32Cfg<FP>::NT)
+__global__ void __launch_bounds__(Fp32Cfg<FP>::NT, Fp32Cfg<FP>::kMinBlocks)
 rows_fp32_kernel(RowsArgs a, int lp_kind) {
   using C = Fp32Cfg<FP>;
   constexpr int KC = C::KC, LDS = C::LDS, NT = C::NT;
@@ -95,13 +98,26 @@ rows_fp32_kernel(RowsArgs a, int lp_kind) {
       }
       __syncthreads();
       if (VEC) {
-        constexpr int C4 = FP / 4;
-        for (int q = tid; q < KC * C4; q += NT) {
-          const int k = q / C4, c4 = q - k * C4;
-          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (k < kc && 4 * c4 < f)
-            v = __ldg(reinterpret_cast<const float4 *>(src + (int64_t)colk[k] * a.ld_src) + c4);
-          reinterpret_cast<float4 *>(th)[q] = v;
+        // A thread's float4 loads of the chunk go out kB at a time, each
+        // batch issued before any of it is stored, so the chunk costs about
+        // kV / kB memory latencies per thread rather than kV (kB is kept small
+        // so the batch fits beside the 8x8 accumulator tile in registers).
+        constexpr int C4 = FP / 4, kV = (KC * C4 + NT - 1) / NT, kB = 3;
+#pragma unroll
+        for (int i0 = 0; i0 < kV; i0 += kB) {
+          float4 v[kB];
+#pragma unroll
+          for (int i = 0; i < kB; ++i) {
+            const int q = tid + (i0 + i) * NT, k = q / C4, c4 = q - k * C4;
+            v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (i0 + i < kV && q < KC * C4 && k < kc && 4 * c4 < f)
+              v[i] = __ldg(reinterpret_cast<const float4 *>(src + (int64_t)colk[k] * a.ld_src) + c4);
+          }
+#pragma unroll
+          for (int i = 0; i < kB; ++i) {
+            const int q = tid + (i0 + i) * NT;
+            if (i0 + i < kV && q < KC * C4) reinterpret_cast<float4 *>(th)[q] = v[i];
+          }
         }
       } else {
         for (int q = tid; q < KC * FP; q += NT) {
