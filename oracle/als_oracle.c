@@ -17,7 +17,7 @@
  *
  * Two modes of the FP64 half-step:
  *   ORC_EXACT   the mathematics the reference intends: symmetric A_u, Cholesky,
- *               x_u = 0 for rows with no ratings. This is the judge of the engine.
+ *               x_u = 0 for rows with no ratings. The engine is checked against this mode.
  *   ORC_REFEMU  reproduces the reference bit for bit where that is defined:
  *               A_u accumulated in FP32 with fused multiply-adds in CSR order
  *               (as the per-thread accumulators temp0..temp99 do), the store
