@@ -79,8 +79,11 @@ enum { ALS_WARM_ZERO = 0, ALS_WARM_PREVIOUS = 1, ALS_WARM_MLP = 2 };
 enum { ALS_SIDE_USERS = 0, ALS_SIDE_ITEMS = 1 };
 
 typedef struct als_options {
-  int32_t precision;    /* ALS_PREC_*: FP32 factors + CUDA-core hermitian, or a
-                           BF16/FP16 factor copy feeding the tensor-core hermitian */
+  int32_t precision;    /* ALS_PREC_*: FP32 factors + CUDA-core hermitian (rank f in
+                           1..128), or a BF16/FP16 factor copy feeding the tensor-core
+                           hermitian (f in 16..128: the warp-specialised persistent
+                           kernel up to 112, a CTA per row above); other ranks give
+                           ALS_ERR_UNSUPPORTED                                    */
   int32_t solver;       /* ALS_SOLVER_*                                          */
   int32_t warm_start;   /* ALS_WARM_* (CG starting point)                        */
   int32_t cg_max_steps; /* default 16                                            */
