@@ -83,3 +83,40 @@ def test_jni_doALSWithCSR_through_fake_env():
     assert err.max() < 1e-3
     X2 = A.do_als_with_csr(ptr32, r.csr_col, r.csr_val, th, r.m, r.n, f, 0.05)
     assert np.array_equal(X, X2)
+
+
+def _no_gpu():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except Exception:
+        return True
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="checks the path taken when no GPU is present")
+def test_jni_without_gpu_returns_null():
+    """Without a usable GPU the entry point reports the CUDA error and returns
+    null, as the reference's catch block does (CuMFJNIInterface.cpp:129-131),
+    instead of ending the executor process."""
+    fk = _fake()
+    f, n, m = 4, 3, 2
+    th = np.arange(n * f, dtype=np.float32).reshape(n, f)
+    outer = fk.fake_object_array(1)
+    blk = fk.fake_object_array(n)
+    keep = [np.ascontiguousarray(th[i]) for i in range(n)]
+    for i, row in enumerate(keep):
+        fk.fake_set(blk, i, fk.fake_float_array(f, row.ctypes.data))
+    fk.fake_set(outer, 0, blk)
+    ptr = np.array([0, 1, 2], np.int32)
+    col = np.array([0, 2], np.int32)
+    val = np.array([4.0, 5.0], np.float32)
+    fn = A.lib.Java_org_apache_spark_ml_recommendation_CuMFJNIInterface_doALSWithCSR
+    fn.restype = ctypes.c_void_p
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.c_void_p, ctypes.c_void_p]
+    out = fn(fk.fake_env(), None, m, n, f, 2, 0.05, outer,
+             fk.fake_int_array(3, ptr.ctypes.data), fk.fake_int_array(2, col.ctypes.data),
+             fk.fake_float_array(2, val.ctypes.data))
+    assert not out
+    assert fk.fake_live_critical() == 0
