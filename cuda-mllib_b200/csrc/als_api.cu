@@ -1,5 +1,6 @@
 // C ABI of the engine: resident model, half-step dispatch, the drop-in
 // doALSWithCSR / utilities entry points, and host-buffer training.
+#include <cuda.h>
 #include <thrust/system/cuda/error.h>
 #include <thrust/system_error.h>
 
@@ -7,9 +8,13 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <iterator>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/als_b200.h"
@@ -80,7 +85,8 @@ struct Side {
   unsigned *queue = nullptr;  // [0]: head, [1..]: order scratch
   uint32_t *flags = nullptr;
   WsPlan plan;                // work list of the warp-specialised kernel
-  void *plan_mem = nullptr;
+  void *plan_mem = nullptr;   // device memory of the plan (plan_ws_bytes for all rows)
+  size_t plan_bytes = 0;
   bool has_plan = false;
 };
 
@@ -257,9 +263,14 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
     return cuda_fail(e, "als_model_create");
   }
   if (kind != kLpNone && tc_ws_supported(f)) {
+    // plan memory for the whole side, so a row range (fewer rows) fits it too
     for (int sd = 0; sd < 2 && e == cudaSuccess; ++sd) {
       Side &S = M->side[sd];
-      e = plan_ws(S.ptr, 0, S.rows, M->num_sms, tc_ws_np(f), (int)S.cols, &S.plan, &S.plan_mem, st);
+      S.plan_bytes = plan_ws_bytes(S.rows, M->num_sms, tc_ws_np(f));
+      e = cudaMalloc(&S.plan_mem, S.plan_bytes);
+      if (e == cudaSuccess)
+        e = plan_ws(S.ptr, 0, S.rows, M->num_sms, tc_ws_np(f), (int)S.cols, S.plan_mem,
+                    S.plan_bytes, &S.plan, &M->ctr->error, st);
       S.has_plan = e == cudaSuccess;
     }
     // the autotuner's candidates are loaded now, so no timed launch pays for it
@@ -415,12 +426,14 @@ int als_model_set_row_range(als_model *M, int32_t side, int64_t begin, int64_t e
   S.active = end - begin;
   ALS_TRY(launch_degree_order(S.ptr, S.active, S.order, S.queue + 1, st, begin), "row range order");
   if (S.has_plan) {
-    cudaFree(S.plan_mem);
-    S.plan_mem = nullptr;
+    // the plan memory is sized for all rows of the side; a launch still
+    // reading the old plan is ordered before this one on the stream
     cudaError_t e = plan_ws(S.ptr, begin, S.active, M->num_sms, tc_ws_np(M->f), (int)S.cols,
-                            &S.plan, &S.plan_mem, st);
-    S.has_plan = e == cudaSuccess;
-    if (e != cudaSuccess) return cuda_fail(e, "row range plan");
+                            S.plan_mem, S.plan_bytes, &S.plan, &M->ctr->error, st);
+    if (e != cudaSuccess) {
+      S.has_plan = false;
+      return cuda_fail(e, "row range plan");
+    }
   }
   return ALS_OK;
 }
@@ -572,7 +585,10 @@ int als_features(int64_t m, int32_t f, const int64_t *ptr, const int32_t *col, c
     // the model's path: a work plan over the rows (long rows split), then the plan kernel
     WsPlan plan;
     void *mem = nullptr;
-    cudaError_t e = plan_ws(ptr, 0, m, device_sm_count(), 128, 0, &plan, &mem, st);
+    const size_t bytes = plan_ws_bytes(m, device_sm_count(), 128);
+    cudaError_t e = cudaMalloc(&mem, bytes);
+    if (e == cudaSuccess)
+      e = plan_ws(ptr, 0, m, device_sm_count(), 128, 0, mem, bytes, &plan, nullptr, st);
     if (e == cudaSuccess) e = mlp_features_plan(plan, f, col, val, src, ld_src, kind, F, ldf, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(mem);
@@ -707,21 +723,124 @@ int als_train(const int64_t *csr_ptr, const int32_t *csr_col, const float *csr_v
   return rc;
 }
 
+}  // extern "C"
+
 // ---------------------------------------------------------------------------
 // Drop-in entry points of the reference.
 // ---------------------------------------------------------------------------
+namespace {
+// Cache of device blocks behind mallocBest / freeBest and the drop-in
+// half-step's workspace. The Spark flow allocates and frees the three CSR
+// arrays and the half-step's scratch on every call (hundreds of MB each at the
+// Netflix shape): cudaMalloc / cudaFree of such blocks take milliseconds each,
+// and cudaFree synchronises the device. A freed block is kept for its device
+// (at most kCacheMax bytes per device; the largest blocks are released first
+// beyond that) and handed out again to a request of at least half its size.
+// When cudaMalloc fails, the device's cached blocks are released and the
+// allocation is tried once more before mallocBest falls back to mapped host
+// memory. The cache is never destroyed: static destructors run after the CUDA
+// runtime may already be gone, and the driver reclaims the memory at exit.
+constexpr size_t kBlockGranule = 2u << 20;
+constexpr size_t kCacheMax = 8ull << 30;
+constexpr int kCacheDevices = 64;
 
-cudaError_t mallocBest(void **devPtr, size_t size) {
-  if (cudaMalloc(devPtr, size) == cudaSuccess) return cudaSuccess;
-  cudaGetLastError();  // clear the allocation failure
-  void *h = nullptr;
-  cudaError_t e = cudaHostAlloc(&h, size, cudaHostAllocMapped | cudaHostAllocWriteCombined);
-  if (e != cudaSuccess) return e;
-  return cudaHostGetDevicePointer(devPtr, h, 0);
+struct BlockCache {
+  std::mutex mu;
+  std::multimap<size_t, void *> idle[kCacheDevices];  // capacity -> block
+  size_t idle_bytes[kCacheDevices] = {};
+  std::unordered_map<void *, std::pair<int, size_t>> live;  // block -> (device, capacity)
+};
+
+BlockCache &block_cache() {
+  static BlockCache *c = new BlockCache();
+  return *c;
 }
 
-cudaError_t freeBest(void *devPtr) {
+// cudaFree of every idle block of device `dev` (the caller holds the lock).
+void release_idle(BlockCache &c, int dev) {
+  for (auto &kv : c.idle[dev]) cudaFree(kv.second);
+  c.idle[dev].clear();
+  c.idle_bytes[dev] = 0;
+}
+
+// A device block of at least `bytes` on the current device.
+cudaError_t block_alloc(void **out, size_t bytes) {
+  *out = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const size_t cap = (std::max<size_t>(bytes, 1) + kBlockGranule - 1) / kBlockGranule * kBlockGranule;
+  BlockCache &c = block_cache();
+  if (dev >= 0 && dev < kCacheDevices) {
+    std::lock_guard<std::mutex> lk(c.mu);
+    auto it = c.idle[dev].lower_bound(cap);
+    if (it != c.idle[dev].end() && it->first / 2 <= cap) {
+      *out = it->second;
+      c.live[it->second] = {dev, it->first};
+      c.idle_bytes[dev] -= it->first;
+      c.idle[dev].erase(it);
+      return cudaSuccess;
+    }
+  }
+  void *p = nullptr;
+  e = cudaMalloc(&p, cap);
+  if (e == cudaErrorMemoryAllocation && dev >= 0 && dev < kCacheDevices) {
+    cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> lk(c.mu);
+      release_idle(c, dev);
+    }
+    e = cudaMalloc(&p, cap);
+  }
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kCacheDevices) {
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.live[p] = {dev, cap};
+  }
+  *out = p;
+  return cudaSuccess;
+}
+
+// Return a block of block_alloc to the cache. false: not such a block. With
+// sync_device, the block's device is synchronised first, as cudaFree would
+// do, so work still queued on it cannot race a later owner.
+bool block_release(void *p, bool sync_device) {
+  BlockCache &c = block_cache();
+  int dev = -1;
+  size_t cap = 0;
+  {
+    std::lock_guard<std::mutex> lk(c.mu);
+    auto it = c.live.find(p);
+    if (it == c.live.end()) return false;
+    dev = it->second.first;
+    cap = it->second.second;
+    c.live.erase(it);
+  }
+  if (sync_device) {
+    int cur = 0;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev) {
+      cudaSetDevice(dev);
+      cudaDeviceSynchronize();
+      cudaSetDevice(cur);
+    } else {
+      cudaDeviceSynchronize();
+    }
+  }
+  std::lock_guard<std::mutex> lk(c.mu);
+  c.idle[dev].insert({cap, p});
+  c.idle_bytes[dev] += cap;
+  while (c.idle_bytes[dev] > kCacheMax && !c.idle[dev].empty()) {
+    auto big = std::prev(c.idle[dev].end());
+    cudaFree(big->second);
+    c.idle_bytes[dev] -= big->first;
+    c.idle[dev].erase(big);
+  }
+  return true;
+}
+
+cudaError_t free_best(void *devPtr, bool sync_device) {
   if (!devPtr) return cudaSuccess;
+  if (block_release(devPtr, sync_device)) return cudaSuccess;
   cudaPointerAttributes attr;
   cudaError_t e = cudaPointerGetAttributes(&attr, devPtr);
   if (e != cudaSuccess) return e;
@@ -729,6 +848,25 @@ cudaError_t freeBest(void *devPtr) {
   // mapped host memory: free through its host address
   return cudaFreeHost(attr.hostPointer ? attr.hostPointer : devPtr);
 }
+}  // namespace
+
+// C++ linkage, as the reference's utilities.h:36-41 declares them.
+cudaError_t mallocBest(void **devPtr, size_t size) {
+  if (!devPtr) return cudaErrorInvalidValue;
+  if (block_alloc(devPtr, size) == cudaSuccess) return cudaSuccess;
+  cudaGetLastError();  // clear the allocation failure
+  void *h = nullptr;
+  cudaError_t e = cudaHostAlloc(&h, size, cudaHostAllocMapped | cudaHostAllocWriteCombined);
+  if (e != cudaSuccess) return e;
+  return cudaHostGetDevicePointer(devPtr, h, 0);
+}
+
+cudaError_t freeBest(void *devPtr) { return free_best(devPtr, true); }
+
+extern "C" {
+
+cudaError_t als_malloc_best(void **devPtr, size_t size) { return mallocBest(devPtr, size); }
+cudaError_t als_free_best(void *devPtr) { return freeBest(devPtr); }
 
 int get_gpu(void) {
   static std::once_flag once;
@@ -751,6 +889,22 @@ static void throw_cuda(cudaError_t e, const char *where) {
   std::fprintf(stderr, "CUDA Error: %s: %s\n", where, cudaGetErrorString(e));
   throw thrust::system_error(e, thrust::cuda_category(), cudaGetErrorString(e));
 }
+
+namespace als {
+// The drop-in call's check of the kernels' error word after a half-step:
+// results of a half-step whose kernel gave up a bounded wait (bit 1), or whose
+// work plan was rejected for malformed row pointers (bit 2), are incomplete,
+// so the call throws like any other CUDA failure instead of returning them.
+void dropin_raise_on_kernel_error(int error_word) {
+  if (error_word == 0) return;
+  const char *what = (error_word & 1)
+                         ? "doALSWithCSR: a kernel gave up a bounded wait (bounded wait timed out); "
+                           "the half-step's rows are incomplete"
+                         : "doALSWithCSR: malformed CSR row pointers; the half-step was not run";
+  std::fprintf(stderr, "CUDA Error: %s\n", what);
+  throw thrust::system_error(cudaErrorLaunchFailure, thrust::cuda_category(), what);
+}
+}  // namespace als
 
 namespace {
 // Host <-> device copies of the drop-in's theta and X. Callers (the JNI shim,
@@ -859,6 +1013,39 @@ cudaError_t staged_copy(void *dst, const void *src, size_t bytes, bool to_device
     if (err[w] != cudaSuccess) return err[w];
   return cudaSuccess;
 }
+
+// The drop-in call's workspace, leased from the block cache and given back
+// when the call ends; on an exception the stream is synchronised first, so no
+// queued kernel still uses the block when the next caller gets it.
+struct WorkspaceLease {
+  char *d = nullptr;
+  cudaStream_t st;
+  explicit WorkspaceLease(cudaStream_t s) : st(s) {}
+  ~WorkspaceLease() {
+    if (!d) return;
+    if (std::uncaught_exceptions() > 0) {
+      cudaStreamSynchronize(st);
+      cudaGetLastError();
+    }
+    block_release(d, false);
+  }
+};
+
+// The CSR arrays the call owns (reference als.cu:1058, 1101-1102): freed on
+// the normal path with their errors checked, and on an exception too (errors
+// ignored) so a failed call does not leak them.
+struct CsrOwnership {
+  void *p[3];
+  cudaStream_t st;
+  bool done = false;
+  ~CsrOwnership() {
+    if (done) return;
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    for (void *q : p) free_best(q, false);
+    cudaGetLastError();
+  }
+};
 }  // namespace
 
 #define DROPIN_CALL(call, where)           \
@@ -871,6 +1058,7 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
                              float *thetaTHost, float *XTHost, const int m, const int n,
                              const int f, const long nnz, const float lambda, const int X_BATCH) {
   (void)X_BATCH;
+  CsrOwnership csr{{csrVal, csrRowIndex, csrColIndex}, st};
   als_options o;
   als_get_dropin_options(&o);
   if (o.warm_start == ALS_WARM_PREVIOUS) o.warm_start = ALS_WARM_ZERO;  // no previous X here
@@ -878,18 +1066,26 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
   if (check_options(o, f) != ALS_OK) throw_cuda(cudaErrorInvalidValue, als_last_error());
   const int kind = lp_kind_of(o.precision);
   const int ldp = kind ? tc_padded_ld(f) : 0;
-  // device buffers: theta (+ low-precision copy), X, widened row pointers, order/queue/counters
+  const int sms = device_sm_count();
+  const bool ws = kind != kLpNone && tc_ws_supported(f) && m > 0;
+  // device buffers: theta (+ low-precision copy), X, widened row pointers,
+  // order/queue/counters, the work plan of the warp-specialised kernel
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t p = off; off = align_up(off + bytes, 256); return p; };
   const size_t oT = take(sizeof(float) * (size_t)n * f), oX = take(sizeof(float) * (size_t)m * f + 4),
                oP = take(sizeof(int64_t) * ((size_t)m + 1)), oW = take(als_half_step_work_bytes(m)),
-               oL = take(kind ? 2ull * n * ldp : 0);
-  char *d = nullptr;
-  DROPIN_CALL(cudaMalloc(&d, off), "doALSWithCSR: cudaMalloc");
+               oL = take(kind ? 2ull * n * ldp : 0),
+               oPl = take(ws ? plan_ws_bytes(m, sms, tc_ws_np(f)) : 0);
+  WorkspaceLease lease(st);
+  void *blk = nullptr;
+  DROPIN_CALL(block_alloc(&blk, off), "doALSWithCSR: workspace");
+  lease.d = static_cast<char *>(blk);
+  char *d = lease.d;
   DROPIN_CALL(staged_copy(d + oT, thetaTHost, sizeof(float) * (size_t)n * f, true, st),
               "doALSWithCSR: theta upload");
   DROPIN_CALL(launch_widen_ptr(csrRowIndex, (int64_t)m + 1, (int64_t *)(d + oP), st),
               "doALSWithCSR: row pointers");
+  int kernel_error = 0;
   if (m > 0 && kind == kLpNone) {
     int rc = als_half_step(m, n, f, (const int64_t *)(d + oP), csrColIndex, csrVal,
                            (const float *)(d + oT), f, (float *)(d + oX), f, lambda, &o, d + oW,
@@ -899,7 +1095,8 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
       throw_cuda(e != cudaSuccess ? e : cudaErrorInvalidValue, als_last_error());
     }
   } else if (m > 0) {
-    // tensor-core form: low-precision copy of theta, a work plan, one launch
+    // tensor-core form: low-precision copy of theta, a work plan built on the
+    // device, one launch
     DROPIN_CALL(launch_convert_lp((const float *)(d + oT), n, f, f, d + oL, ldp, kind, st),
                 "doALSWithCSR: theta copy");
     Side S;
@@ -911,26 +1108,28 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
     Counters *ctr = (Counters *)((char *)S.queue + align_up(sizeof(unsigned) * (1 + 3 * kOrderBins), 256));
     DROPIN_CALL(cudaMemsetAsync(ctr, 0, sizeof(Counters), st), "doALSWithCSR: counters");
     DROPIN_CALL(launch_degree_order(S.ptr, m, S.order, S.queue + 1, st), "doALSWithCSR: order");
-    if (tc_ws_supported(f)) {
-      DROPIN_CALL(plan_ws(S.ptr, 0, m, device_sm_count(), tc_ws_np(f), n, &S.plan, &S.plan_mem, st),
+    if (ws) {
+      DROPIN_CALL(plan_ws(S.ptr, 0, m, sms, tc_ws_np(f), n, d + oPl, plan_ws_bytes(m, sms, tc_ws_np(f)),
+                          &S.plan, &ctr->error, st),
                   "doALSWithCSR: plan");
       S.has_plan = true;
     }
-    cudaError_t e = run_rows(S, f, lambda, o, (const float *)(d + oT), f, d + oL, ldp,
-                             (float *)(d + oX), nullptr, ctr, nullptr, device_sm_count(), st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(S.plan_mem);
-    if (e != cudaSuccess) throw_cuda(e, "doALSWithCSR: tensor-core half-step");
+    DROPIN_CALL(run_rows(S, f, lambda, o, (const float *)(d + oT), f, d + oL, ldp, (float *)(d + oX),
+                         nullptr, ctr, nullptr, sms, st),
+                "doALSWithCSR: tensor-core half-step");
+    DROPIN_CALL(cudaMemcpyAsync(&kernel_error, &ctr->error, sizeof(int), cudaMemcpyDeviceToHost, st),
+                "doALSWithCSR: error word");
   }
   if (m > 0)
     DROPIN_CALL(staged_copy(XTHost, d + oX, sizeof(float) * (size_t)m * f, false, st),
                 "doALSWithCSR: X download");
   DROPIN_CALL(cudaStreamSynchronize(st), "doALSWithCSR: sync");
-  DROPIN_CALL(cudaFree(d), "doALSWithCSR: cudaFree");
+  dropin_raise_on_kernel_error(kernel_error);
   // The callee owns and frees the CSR arrays (reference als.cu:1058, 1101-1102).
-  DROPIN_CALL(freeBest(csrVal), "doALSWithCSR: free csrVal");
-  DROPIN_CALL(freeBest(csrRowIndex), "doALSWithCSR: free csrRowIndex");
-  DROPIN_CALL(freeBest(csrColIndex), "doALSWithCSR: free csrColIndex");
+  csr.done = true;
+  DROPIN_CALL(free_best(csrVal, false), "doALSWithCSR: free csrVal");
+  DROPIN_CALL(free_best(csrRowIndex, false), "doALSWithCSR: free csrRowIndex");
+  DROPIN_CALL(free_best(csrColIndex, false), "doALSWithCSR: free csrColIndex");
 }
 
 // ---------------------------------------------------------------------------
@@ -953,22 +1152,61 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 namespace {
 constexpr int kStaticMaxDevices = 64;
 std::mutex g_static_mu;
-void *g_static_ptr[kStaticMaxDevices];
+struct StaticScratchEntry {
+  void *ptr = nullptr;
+  unsigned long long ctx = 0;  // context the address belongs to (0: unknown)
+};
+StaticScratchEntry g_static[kStaticMaxDevices];
 
-// Device address of the scratch array on the current device, looked up with
-// cudaGetSymbolAddress the first time a call runs on that device.
+// ID of the calling thread's current context (cuCtxGetId, unique within the
+// process), or 0 when it cannot be read. The driver functions are reached
+// through the runtime's entry-point query, so the library needs no link to
+// the driver library.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(fn);
+    fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(fn);
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
+
+// Device address of the scratch array in the current device's context,
+// looked up with cudaGetSymbolAddress the first time a call runs in that
+// context. A device reset (or a released and re-created primary context)
+// reloads the module at a new address; the context ID tells the cached
+// address apart from the new one, so the lookup is repeated then.
 int static_scratch(void **out) {
   int dev = 0;
   ALS_TRY(cudaGetDevice(&dev), "als_half_step_static: cudaGetDevice");
   if (dev < 0 || dev >= kStaticMaxDevices)
     return fail(ALS_ERR_UNSUPPORTED, "als_half_step_static: device ordinal above 63");
   std::lock_guard<std::mutex> lk(g_static_mu);
-  if (!g_static_ptr[dev]) {
+  StaticScratchEntry &ent = g_static[dev];
+  const unsigned long long ctx = current_context_id();
+  if (!ent.ptr || ctx == 0 || ctx != ent.ctx) {
     void *p = nullptr;
     ALS_TRY(cudaGetSymbolAddress(&p, g_static_scratch), "als_half_step_static: cudaGetSymbolAddress");
-    g_static_ptr[dev] = p;
+    ent.ptr = p;
+    ent.ctx = current_context_id();  // the lookup has made the context current
   }
-  *out = g_static_ptr[dev];
+  *out = ent.ptr;
   return ALS_OK;
 }
 }  // namespace

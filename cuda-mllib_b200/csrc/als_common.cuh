@@ -31,7 +31,8 @@ struct Counters {
   unsigned long long cg_steps;
   unsigned long long cg_fallback;
   unsigned long long r0_micro;  // sum over CG rows of |b - A x0| / |b| (after scaling), x 1e6
-  int error;             // sticky kernel error code (1: a bounded wait timed out)
+  int error;             // sticky kernel error bits (1: a bounded wait timed out,
+                         // 2: row pointers malformed beyond the work plan's bounds)
   int pad;
 };
 

@@ -50,7 +50,8 @@ constexpr int kCholFloats = 112 * 113;
 
 struct WsPlan {
   const WorkItem *items = nullptr;
-  int nitems = 0;
+  int nitems = 0;                      // items, or (with nitems_dev) an upper bound
+  const int *nitems_dev = nullptr;     // the exact item count, in device memory
   const int *heavy_nchunks = nullptr;  // per split row: number of chunks
   const int *heavy_base = nullptr;     // per split row: first partial slot
   unsigned *heavy_count = nullptr;     // per split row: chunks finished (reset by the last)
@@ -61,11 +62,17 @@ struct WsPlan {
   int ctas = 0;                        // CTAs the scratch covers: a launch uses at most this many
 };
 
-// Host-side planning of a side's rows [begin, begin + count): items sorted by
-// size, rows above `split` ratings cut into chunks. Device buffers are
-// allocated into `plan` and `mem` (freed with cudaFree(*mem)).
+// Planning of a side's rows [begin, begin + count) on the device (no host
+// copy, no synchronisation): items sorted by size bin, largest first, rows
+// above `split` ratings cut into chunks, dealt to min(grid, count) CTAs. The
+// plan lives in caller memory of plan_ws_bytes() bytes (256-byte aligned),
+// which must stay untouched while the plan is used. `error` (may be null) is
+// set when the row pointers are malformed beyond the plan's bounds; the plan
+// is then empty.
+size_t plan_ws_bytes(int64_t count, int grid, int np);
 cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int grid, int np,
-                    int src_rows, WsPlan *plan, void **mem, cudaStream_t st);
+                    int src_rows, void *mem, size_t mem_bytes, WsPlan *plan, int *error,
+                    cudaStream_t st);
 
 // Warp-specialised tensor-core kernel (f in [16, 112]); launch_rows_tc
 // dispatches to it when a plan is given.

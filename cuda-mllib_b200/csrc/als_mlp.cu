@@ -362,7 +362,8 @@ __global__ void __launch_bounds__(256) features_plan_kernel(WsPlan plan, int f, 
   __shared__ int last;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, h = lane >> 4, j = lane & 15;
   const int nj = ld_src / 8;
-  for (int64_t idx = blockIdx.x; idx < plan.nitems; idx += gridDim.x) {
+  const int64_t nitems = plan.nitems_dev ? *plan.nitems_dev : plan.nitems;
+  for (int64_t idx = blockIdx.x; idx < nitems; idx += gridDim.x) {
     const WorkItem it = plan.items[idx];
     const int64_t S0 = it.s, E0 = it.e;
     float b[8], d[8];

@@ -861,7 +861,7 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
 
 template <int FP, int NP, typename LP, int NG>
 __global__ void __launch_bounds__(ws::threads<NG>(), 1)
-rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan) {
+rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_arg) {
   using L = WsLayout<FP, NP, NG>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char *base = smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023);
@@ -878,6 +878,8 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan)
   c.row_info = c.stage_info + ws::NS;
   c.misc = reinterpret_cast<volatile int *>(c.row_info + ws::kRowSlots);
   const int tid = threadIdx.x, warp = tid >> 5;
+  WsPlan plan = plan_arg;
+  if (plan.nitems_dev) plan.nitems = *plan.nitems_dev;  // built on the device
 
   if (tid == 0) {
     for (int i = 0; i < ws::NS; ++i) {
@@ -965,8 +967,8 @@ static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
   auto kern = rows_tc_ws_kernel<FP, NP, LP, NG>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kTotal);
   if (err != cudaSuccess || sv.prepare) return err;
-  int64_t grid = std::min(num_sms, plan.ctas);
-  if (grid > plan.nitems) grid = plan.nitems > 0 ? plan.nitems : 1;
+  (void)num_sms;
+  const int grid = plan.ctas;  // the items were dealt to exactly this many CTAs
   if (grid < 1 || !plan.chol) return cudaErrorInvalidValue;
   const int nmma = ((std::max(NP, a.ld_src + 1) + 15) / 16) * 16;  // B columns incl. c_r
   const uint32_t idesc = tc::make_idesc(lp_kind == kLpBf16 ? 1 : 0, nmma);
@@ -1008,151 +1010,277 @@ cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
 }
 
 // ---------------------------------------------------------------------------
-// host planning of the work list
+// device planning of the work list
 // ---------------------------------------------------------------------------
+// The work list of a side is built on the device from its row pointers, with
+// no copy to the host and no synchronisation:
+//   plan_count_kernel  per row: its item count (1, or the chunks of a row
+//                      longer than `split`), a histogram of item sizes over
+//                      kPlanBins size bins (largest first), and for each split
+//                      row its chunk count and first partial slot;
+//   plan_scan_kernel   exclusive scan of the histogram (the first rank of each
+//                      bin) and the item total;
+//   plan_place_kernel  each item's rank (its bin's next free rank: a block
+//                      reserves its bin counts in one atomic per bin, then
+//                      ranks its rows in shared memory) and its place: rank k
+//                      goes to CTA k mod G, and within the CTA the order zigzags
+//                      between its largest and smallest items, so rows that load
+//                      the producers (many ratings) alternate with rows that
+//                      load the solvers (few ratings).
+// Items of one size bin are ranked in no fixed order; every row is solved the
+// same way wherever it is placed (the partial sums of a split row are added in
+// chunk order), so the results do not depend on the order.
 namespace {
-// Host memory of the planner (the row pointers read back and the item list
-// before its upload), kept across calls: a fresh allocation costs one page
-// fault per 4 KB on first touch, which at the Netflix shape (19 MB) took
-// longer than the planning itself. Pinned when the driver grants it, so the
-// upload is one DMA. Guarded by plan_host_mu; every plan_ws call synchronises
-// its stream before it lets go, so no copy from it is in flight then.
-std::mutex plan_host_mu;
-char *plan_host = nullptr;
-size_t plan_host_cap = 0;
-bool plan_host_pinned = false;
+constexpr int kPlanBins = 4096;
+constexpr int kPlanThreads = 512;
 
-char *plan_host_buffer(size_t bytes) {
-  if (bytes <= plan_host_cap) return plan_host;
-  if (plan_host) {
-    if (plan_host_pinned) cudaFreeHost(plan_host);
-    else std::free(plan_host);
+struct PlanHdr {
+  unsigned long long extra;  // items beyond one per row (extra chunks of split rows)
+  int nheavy, nslots, nitems, pad;
+};
+
+struct PlanDev {
+  const int64_t *ptr;
+  int64_t begin, count;
+  int grid, hmax, smax;
+  int64_t imax;  // capacity of items
+  int *error;  // optional: bit 2 set when the row pointers break the bounds below
+  PlanHdr *hdr;
+  unsigned *hist, *cursor;
+  int *heavy_row, *heavy_nchunks, *heavy_base;
+  unsigned *heavy_count;
+  WorkItem *items;
+};
+
+__device__ __forceinline__ int64_t plan_split(const PlanDev &p) {
+  const int64_t nnz = p.ptr[p.begin + p.count] - p.ptr[p.begin];
+  const int64_t q = 4LL * p.grid;
+  const int64_t s = (nnz + q - 1) / q;
+  return s > 8192 ? s : 8192;
+}
+static_assert(kPlanBins == 4 * 1024, "plan_scan_kernel: 1024 threads of four bins");
+
+// A row's rating count; a decreasing row pointer (a malformed CSR) counts as
+// an empty row rather than a negative size.
+__device__ __forceinline__ int64_t plan_deg(const PlanDev &p, int64_t r) {
+  const int64_t d = p.ptr[p.begin + r + 1] - p.ptr[p.begin + r];
+  return d > 0 ? d : 0;
+}
+__device__ __forceinline__ int plan_bin(int64_t size, int64_t split) {
+  return (int)((split - size) * kPlanBins / (split + 1));
+}
+__device__ __forceinline__ void plan_rows_of_block(const PlanDev &p, int64_t &r0, int64_t &r1) {
+  const int64_t per = (p.count + gridDim.x - 1) / gridDim.x;
+  r0 = (int64_t)blockIdx.x * per;
+  r1 = r0 + per < p.count ? r0 + per : p.count;
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_count_kernel(PlanDev p) {
+  __shared__ unsigned hs[kPlanBins];
+  for (int b = threadIdx.x; b < kPlanBins; b += blockDim.x) hs[b] = 0;
+  __syncthreads();
+  const int64_t split = plan_split(p);
+  int64_t r0, r1;
+  plan_rows_of_block(p, r0, r1);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    const int64_t d = plan_deg(p, r);
+    if (d > split) {
+      const int64_t nch = (d + split - 1) / split;
+      atomicAdd(&hs[0], (unsigned)(nch - 1));  // full chunks
+      atomicAdd(&hs[plan_bin(d - (nch - 1) * split, split)], 1u);
+      const int h = atomicAdd(&p.hdr->nheavy, 1);
+      const int hb = atomicAdd(&p.hdr->nslots, (int)nch);
+      if (h >= p.hmax || hb + nch > p.smax) {  // only a malformed CSR gets here
+        p.hdr->pad = 1;
+        continue;
+      }
+      p.heavy_row[h] = (int)r;
+      p.heavy_nchunks[h] = (int)nch;
+      p.heavy_base[h] = hb;
+      p.heavy_count[h] = 0;
+      atomicAdd(&p.hdr->extra, (unsigned long long)(nch - 1));
+    } else {
+      atomicAdd(&hs[plan_bin(d, split)], 1u);
+    }
   }
-  plan_host_cap = 0;
-  const size_t want = bytes + bytes / 4;
-  plan_host_pinned = cudaHostAlloc((void **)&plan_host, want, cudaHostAllocPortable) == cudaSuccess;
-  if (!plan_host_pinned) {
-    cudaGetLastError();
-    plan_host = static_cast<char *>(std::malloc(want));
-    if (!plan_host) return nullptr;
+  __syncthreads();
+  for (int b = threadIdx.x; b < kPlanBins; b += blockDim.x)
+    if (hs[b]) atomicAdd(&p.hist[b], hs[b]);
+}
+
+// One block of 1024 threads: each scans four consecutive bins.
+__global__ void __launch_bounds__(1024) plan_scan_kernel(PlanDev p) {
+  __shared__ unsigned part[1024];
+  const int t = threadIdx.x;
+  unsigned v[4], s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = p.hist[4 * t + k];
+    s += v[k];
   }
-  plan_host_cap = want;
-  return plan_host;
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const unsigned add = t >= o ? part[t - o] : 0u;
+    __syncthreads();
+    part[t] += add;
+    __syncthreads();
+  }
+  unsigned run = part[t] - s;  // exclusive prefix of this thread's four bins
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    p.cursor[4 * t + k] = run;
+    run += v[k];
+  }
+  if (t == 0) {
+    // Row pointers that broke the plan's bounds leave no plan at all
+    // (nothing is solved) and raise the error word, rather than a partial one.
+    const int64_t n = p.count + (int64_t)p.hdr->extra;
+    const bool bad = p.hdr->pad != 0 || n > p.imax;
+    p.hdr->nitems = bad ? 0 : (int)n;
+    if (bad && p.error) atomicOr(p.error, 2);
+  }
+}
+
+__device__ __forceinline__ void plan_put(const PlanDev &p, int64_t k, int64_t N, const WorkItem &w) {
+  const int64_t G = p.grid, c = k % G, q = k / G, nc = (N - c + G - 1) / G;
+  const int64_t j = q < (nc + 1) / 2 ? 2 * q : 2 * (nc - 1 - q) + 1;  // zigzag slot
+  p.items[c + j * G] = w;
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_place_kernel(PlanDev p) {
+  __shared__ unsigned cnt[kPlanBins];
+  __shared__ unsigned base[kPlanBins];
+  for (int b = threadIdx.x; b < kPlanBins; b += blockDim.x) cnt[b] = 0;
+  __syncthreads();
+  const int64_t split = plan_split(p), N = p.hdr->nitems;
+  if (N == 0) return;  // a rejected plan (block-uniform)
+  int64_t r0, r1;
+  plan_rows_of_block(p, r0, r1);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    const int64_t d = plan_deg(p, r);
+    if (d <= split) atomicAdd(&cnt[plan_bin(d, split)], 1u);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < kPlanBins; b += blockDim.x) {
+    base[b] = cnt[b] ? atomicAdd(&p.cursor[b], cnt[b]) : 0u;
+    cnt[b] = 0;
+  }
+  __syncthreads();
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    const int64_t s = p.ptr[p.begin + r], d = plan_deg(p, r);
+    if (d > split) continue;
+    const int b = plan_bin(d, split);
+    WorkItem w;
+    w.s = s;
+    w.e = s + d;
+    w.u = (int)(p.begin + r);
+    w.deg = (int)d;
+    w.part = -1;
+    w.heavy = -1;
+    plan_put(p, (int64_t)base[b] + atomicAdd(&cnt[b], 1u), N, w);
+  }
+  // the chunks of split rows, a split row per block at a time
+  const int nheavy = p.hdr->nheavy;
+  for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
+    const int64_t r = p.heavy_row[h], s = p.ptr[p.begin + r], e = s + plan_deg(p, r);
+    const int nch = p.heavy_nchunks[h], hb = p.heavy_base[h];
+    for (int ch = threadIdx.x; ch < nch; ch += blockDim.x) {
+      WorkItem w;
+      w.s = s + ch * split;
+      w.e = min(e, s + (ch + 1) * split);
+      w.u = (int)(p.begin + r);
+      w.deg = (int)(e - s);
+      w.part = hb + ch;
+      w.heavy = h;
+      plan_put(p, (int64_t)atomicAdd(&p.cursor[plan_bin(w.e - w.s, split)], 1u), N, w);
+    }
+  }
+}
+
+struct PlanLayout {
+  size_t oHdr, oHist, oCur, oHr, oHn, oHb, oHc, oItems, oPart, oChol, total;
+  PlanLayout(int64_t count, int grid, int np) {
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    // A row of d > split ratings becomes ceil(d / split) < d / split + 1
+    // chunks, and split >= nnz / (4 grid): fewer than 4 grid split rows,
+    // fewer than 8 grid chunks of them, fewer than count + 4 grid items.
+    const size_t hmax = 4 * (size_t)grid + 1, smax = 8 * (size_t)grid,
+                 imax = (size_t)count + 4 * (size_t)grid;
+    size_t o = 0;
+    oHdr = o; o += al(sizeof(PlanHdr));
+    oHist = o; o += al(4 * kPlanBins);
+    oCur = o; o += al(4 * kPlanBins);
+    oHr = o; o += al(4 * hmax);
+    oHn = o; o += al(4 * hmax);
+    oHb = o; o += al(4 * hmax);
+    oHc = o; o += al(4 * hmax);
+    oItems = o; o += al(sizeof(WorkItem) * imax);
+    oPart = o; o += al(sizeof(float) * smax * 128 * (size_t)(np + 4) + 16);
+    oChol = o; o += al(sizeof(float) * (size_t)grid * ws::kMaxGroups * kCholFloats);
+    total = o;
+  }
+};
+
+int plan_grid(int64_t count, int grid) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>(grid, count));
 }
 }  // namespace
 
+size_t plan_ws_bytes(int64_t count, int grid, int np) {
+  return PlanLayout(count, plan_grid(count, grid), np).total;
+}
+
 cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int grid, int np,
-                    int src_rows, WsPlan *plan, void **mem, cudaStream_t st) {
-  *mem = nullptr;
+                    int src_rows, void *mem, size_t mem_bytes, WsPlan *plan, int *error,
+                    cudaStream_t st) {
   *plan = WsPlan();
   plan->src_rows = src_rows;
   plan->part_ld = np + 4;
   if (count <= 0) return cudaSuccess;
-  std::lock_guard<std::mutex> lk(plan_host_mu);
-  // A row of d > split ratings becomes ceil(d / split) <= d / split + 1
-  // chunks and split >= nnz / (4 grid), so there are at most count + 4 grid
-  // items.
-  const size_t ptr_bytes = (sizeof(int64_t) * ((size_t)count + 1) + 255) / 256 * 256;
-  char *host = plan_host_buffer(ptr_bytes + sizeof(WorkItem) * ((size_t)count + 4 * (size_t)grid));
-  if (!host) return cudaErrorMemoryAllocation;
-  int64_t *ptr = reinterpret_cast<int64_t *>(host);
-  WorkItem *out = reinterpret_cast<WorkItem *>(host + ptr_bytes);
-  cudaError_t e = cudaMemcpyAsync(ptr, d_row_ptr + begin, sizeof(int64_t) * (count + 1),
-                                  cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (count > INT32_MAX) return cudaErrorInvalidValue;
+  // Every CTA of the launch gets at least one item: there are at least as
+  // many items as rows.
+  grid = plan_grid(count, grid);
+  const PlanLayout L(count, grid, np);
+  if (!mem || mem_bytes < L.total || (reinterpret_cast<uintptr_t>(mem) & 255) != 0)
+    return cudaErrorInvalidValue;
+  char *d = static_cast<char *>(mem);
+  PlanDev p;
+  p.ptr = d_row_ptr;
+  p.begin = begin;
+  p.count = count;
+  p.grid = grid;
+  p.hmax = 4 * grid + 1;
+  p.smax = 8 * grid;
+  p.imax = count + 4LL * grid;
+  p.error = error;
+  p.hdr = reinterpret_cast<PlanHdr *>(d + L.oHdr);
+  p.hist = reinterpret_cast<unsigned *>(d + L.oHist);
+  p.cursor = reinterpret_cast<unsigned *>(d + L.oCur);
+  p.heavy_row = reinterpret_cast<int *>(d + L.oHr);
+  p.heavy_nchunks = reinterpret_cast<int *>(d + L.oHn);
+  p.heavy_base = reinterpret_cast<int *>(d + L.oHb);
+  p.heavy_count = reinterpret_cast<unsigned *>(d + L.oHc);
+  p.items = reinterpret_cast<WorkItem *>(d + L.oItems);
+  cudaError_t e = cudaMemsetAsync(d, 0, L.oCur, st);  // header and histogram
   if (e != cudaSuccess) return e;
-  const int64_t nnz = ptr[(size_t)count] - ptr[0];
-  // rows longer than a quarter of a CTA's fair share are split
-  const int64_t split = std::max<int64_t>(8192, (nnz + 4LL * grid - 1) / (4LL * grid));
-  // Order: largest item first, ties in row order (a stable counting sort on
-  // the item size, at most `split` ratings), then dealt to CTAs round robin
-  // (CTA c takes sorted items c, c + grid, ...: balanced by the sort). Within
-  // a CTA the order zigzags between its largest and smallest items, so rows
-  // that load the producers (many ratings) alternate with rows that load the
-  // solvers (few ratings) instead of coming in two long runs. Both steps are
-  // a position per item: one pass counts, the second writes each item once
-  // to its final place.
-  std::vector<int64_t> start((size_t)split + 2, 0);
-  std::vector<int> hn, hb;
-  int slots = 0;
-  int64_t N = 0;
-  for (int64_t r = 0; r < count; ++r) {
-    const int64_t d = ptr[(size_t)r + 1] - ptr[(size_t)r];
-    if (d > split) {
-      const int64_t nch = (d + split - 1) / split;
-      start[0] += nch - 1;  // full chunks
-      ++start[(size_t)(split - (d - (nch - 1) * split))];
-      hn.push_back((int)nch);
-      hb.push_back(slots);
-      slots += (int)nch;
-      N += nch;
-    } else {
-      ++start[(size_t)(split - d)];
-      ++N;
-    }
-  }
-  {
-    int64_t acc = 0;
-    for (auto &v : start) {
-      const int64_t c = v;
-      v = acc;
-      acc += c;
-    }
-  }
-  const int64_t G = grid;
-  auto place = [&](const WorkItem &w) {
-    const int64_t k = start[(size_t)(split - (w.e - w.s))]++;  // rank, largest first
-    const int64_t c = k % G, q = k / G, nc = (N - c + G - 1) / G;
-    const int64_t j = q < (nc + 1) / 2 ? 2 * q : 2 * (nc - 1 - q) + 1;  // zigzag slot
-    out[(size_t)(c + j * G)] = w;
-  };
-  for (int64_t r = 0, h = 0; r < count; ++r) {
-    const int64_t s = ptr[(size_t)r], e2 = ptr[(size_t)r + 1], d = e2 - s;
-    WorkItem w;
-    w.u = (int)(begin + r);
-    w.deg = (int)d;
-    if (d > split) {
-      for (int ch = 0; ch < hn[(size_t)h]; ++ch) {
-        w.s = s + ch * split;
-        w.e = std::min<int64_t>(e2, s + (ch + 1) * split);
-        w.part = hb[(size_t)h] + ch;
-        w.heavy = (int)h;
-        place(w);
-      }
-      ++h;
-    } else {
-      w.s = s;
-      w.e = e2;
-      w.part = -1;
-      w.heavy = -1;
-      place(w);
-    }
-  }
-  const size_t nh = hn.size();
-  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-  const size_t oI = 0, oN = al(sizeof(WorkItem) * (size_t)N), oB = oN + al(4 * (nh + 1)),
-               oC = oB + al(4 * (nh + 1)), oP = oC + al(4 * (nh + 1)),
-               oK = oP + al(sizeof(float) * (size_t)slots * 128 * plan->part_ld + 16),
-               total = oK + al(sizeof(float) * (size_t)grid * ws::kMaxGroups * kCholFloats);
-  char *d = nullptr;
-  if ((e = cudaMalloc(&d, total)) != cudaSuccess) return e;
-  e = cudaMemcpyAsync(d + oI, out, sizeof(WorkItem) * (size_t)N, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && nh)
-    e = cudaMemcpyAsync(d + oN, hn.data(), 4 * nh, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && nh)
-    e = cudaMemcpyAsync(d + oB, hb.data(), 4 * nh, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d + oC, 0, 4 * (nh + 1), st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host memory is reused after this
-  if (e != cudaSuccess) { cudaFree(d); return e; }
-  plan->items = (const WorkItem *)(d + oI);
-  plan->nitems = (int)N;
-  plan->heavy_nchunks = (const int *)(d + oN);
-  plan->heavy_base = (const int *)(d + oB);
-  plan->heavy_count = (unsigned *)(d + oC);
-  plan->partial = (float *)(d + oP);
-  plan->chol = (float *)(d + oK);
+  const int sms = device_sm_count();
+  const unsigned blocks = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(2LL * (sms > 0 ? sms : 148), (count + kPlanThreads - 1) / kPlanThreads));
+  plan_count_kernel<<<blocks, kPlanThreads, 0, st>>>(p);
+  plan_scan_kernel<<<1, 1024, 0, st>>>(p);
+  plan_place_kernel<<<blocks, kPlanThreads, 0, st>>>(p);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  plan->items = p.items;
+  plan->nitems = (int)std::min<int64_t>(INT32_MAX, count + 4LL * grid);  // upper bound
+  plan->nitems_dev = &p.hdr->nitems;
+  plan->heavy_nchunks = p.heavy_nchunks;
+  plan->heavy_base = p.heavy_base;
+  plan->heavy_count = p.heavy_count;
+  plan->partial = reinterpret_cast<float *>(d + L.oPart);
+  plan->chol = reinterpret_cast<float *>(d + L.oChol);
   plan->ctas = grid;
-  *mem = d;
   return cudaSuccess;
 }
 

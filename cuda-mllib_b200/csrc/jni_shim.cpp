@@ -116,11 +116,24 @@ extern "C" jobjectArray Java_org_apache_spark_ml_recommendation_CuMFJNIInterface
     if (index != (size_t)n)
       throw thrust::system_error(cudaErrorInvalidValue, thrust::cuda_category(),
                                  "source factor count differs from n");
-    int *d_row = nullptr, *d_col = nullptr;
-    float *d_val = nullptr;
-    check(mallocBest((void **)&d_row, sizeof(int) * ((size_t)m + 1)), "mallocBest row");
-    check(mallocBest((void **)&d_col, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)), "mallocBest col");
-    check(mallocBest((void **)&d_val, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1)), "mallocBest val");
+    // The CSR arrays go to doALSWithCSR, which frees them; until then they
+    // are this call's, and a failure before the hand-over frees them here.
+    struct CsrArrays {
+      int *row = nullptr, *col = nullptr;
+      float *val = nullptr;
+      bool handed_over = false;
+      ~CsrArrays() {
+        if (handed_over) return;
+        freeBest(row);
+        freeBest(col);
+        freeBest(val);
+      }
+    } csr;
+    check(mallocBest((void **)&csr.row, sizeof(int) * ((size_t)m + 1)), "mallocBest row");
+    check(mallocBest((void **)&csr.col, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)), "mallocBest col");
+    check(mallocBest((void **)&csr.val, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1)), "mallocBest val");
+    int *d_row = csr.row, *d_col = csr.col;
+    float *d_val = csr.val;
     void *hr = J.GetPrimitiveArrayCritical(csrRow, nullptr);
     void *hc = J.GetPrimitiveArrayCritical(csrCol, nullptr);
     void *hv = J.GetPrimitiveArrayCritical(csrVal, nullptr);
@@ -134,6 +147,7 @@ extern "C" jobjectArray Java_org_apache_spark_ml_recommendation_CuMFJNIInterface
     J.ReleasePrimitiveArrayCritical(csrCol, hc, 0);
     J.ReleasePrimitiveArrayCritical(csrVal, hv, 0);
     check(e, "CSR upload");
+    csr.handed_over = true;  // doALSWithCSR frees them, on success and on failure
     doALSWithCSR(stream, d_row, d_col, d_val, thetaTHost, XTHost, m, n, f, nnz, (float)lambda, 1);
     jclass floatArrayClass = J.FindClass("[F");
     jobjectArray output = J.NewObjectArray(m, floatArrayClass, nullptr);

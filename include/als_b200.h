@@ -7,8 +7,8 @@
  *     (IBMSparkGPU/CUDA-MLlib), so an existing caller links unchanged:
  *       doALSWithCSR   replaces als/src/cuda/als.h:96-103 (body als.cu:1001-1115)
  *       get_gpu        replaces utilities.h:39 (body utilities.cu:97-136)
- *       mallocBest     replaces utilities.h:40 (body utilities.cu:73-82)
- *       freeBest       replaces utilities.h:41 (body utilities.cu:85-95)
+ *       mallocBest     replaces utilities.h:40 (body utilities.cu:73-82), C++ linkage
+ *       freeBest       replaces utilities.h:41 (body utilities.cu:85-95), C++ linkage
  *     The Spark JNI symbols of als/src/org_apache_spark_ml_recommendation_CuMFJNIInterface.h:31-40
  *     are exported from the same library (see cumf_jni.h).
  *
@@ -58,10 +58,24 @@ void doALSWithCSR(cudaStream_t cuda_stream, int *csrRowIndex, int *csrColIndex, 
  * does not reset every device on first use, which would destroy contexts that
  * other libraries in the same process hold. Returns -1 without devices. */
 int get_gpu(void);
-/* cudaMalloc, falling back to mapped pinned host memory (utilities.cu:73-82). */
+
+/* cudaMalloc, falling back to mapped pinned host memory (utilities.cu:73-82),
+ * and the free of either kind of such allocation (utilities.cu:85-95).
+ * The reference's utilities.h:36-41 gives C linkage to get_gpu only, so its
+ * C++ callers (CuMFJNIInterface.cpp:93-95) bind the C++ names
+ * mallocBest(void**, size_t) and freeBest(void*): those are declared below,
+ * outside the extern "C" block, with the same linkage. C and FFI callers
+ * (ctypes, cgo) use the C-linkage aliases als_malloc_best / als_free_best,
+ * which are the same functions. */
+cudaError_t als_malloc_best(void **devPtr, size_t size);
+cudaError_t als_free_best(void *devPtr);
+
+#ifdef __cplusplus
+} /* extern "C" */
 cudaError_t mallocBest(void **devPtr, size_t size);
-/* Frees either kind of mallocBest allocation (utilities.cu:85-95). */
 cudaError_t freeBest(void *devPtr);
+extern "C" {
+#endif
 
 /* ---------------- 2. engine API ---------------- */
 
@@ -193,8 +207,10 @@ int als_half_step(int64_t m, int64_t n, int32_t f, const int64_t *d_row_ptr,
  * library until the process exits), so a call allocates nothing.
  * Larger m is rejected with ALS_ERR_INVALID. The first call on each device
  * looks the array up with cudaGetSymbolAddress; make that first call before
- * any stream capture. Calls that overlap in time (two streams, two host
- * threads) share the one array and race: serialise them.
+ * any stream capture. After a device reset (which reloads the library's
+ * device code at a new address) the next call looks it up again, so that
+ * call too belongs before any capture. Calls that overlap in time (two
+ * streams, two host threads) share the one array and race: serialise them.
  * No counterpart in the reference. */
 #define ALS_STATIC_MAX_ROWS 1048576
 int als_half_step_static(int64_t m, int64_t n, int32_t f, const int64_t *d_row_ptr,

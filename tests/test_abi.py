@@ -4,6 +4,7 @@ without touching a GPU."""
 import ctypes
 import os
 import re
+import subprocess
 
 import pytest
 
@@ -13,8 +14,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INC = os.path.join(ROOT, "include")
 
 
+# Declared with C++ linkage, as the reference's utilities.h:36-41 does; their
+# exported names are mangled (checked by test_cxx_linkage_names).
+CXX_LINKAGE = {"mallocBest": "_Z10mallocBestPPvm", "freeBest": "_Z8freeBestPv"}
+
+
 def _declared(header):
     text = open(os.path.join(INC, header)).read()
+    # the block of C++-linkage declarations
+    text = re.sub(r"#ifdef __cplusplus\n\} /\* extern \"C\" \*/.*?#endif", "", text, flags=re.S)
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     names = set()
     for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text):
@@ -44,10 +52,45 @@ def test_every_declared_symbol_is_exported(header, libattr):
 
 
 def test_dropin_symbols_match_reference_names():
-    for n in ("doALSWithCSR", "get_gpu", "mallocBest", "freeBest",
+    for n in ("doALSWithCSR", "get_gpu", "als_malloc_best", "als_free_best",
               "Java_org_apache_spark_ml_recommendation_CuMFJNIInterface_doALSWithCSR",
               "Java_org_apache_spark_ml_recommendation_CuMFJNIInterface_testjni"):
         assert hasattr(A.lib, n)
+    for n in CXX_LINKAGE:  # C++ linkage only: no C name
+        assert not hasattr(A.lib, n)
+
+
+def _dynsyms(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", path], check=True, capture_output=True,
+                         text=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+def test_cxx_linkage_names():
+    syms = _dynsyms(os.path.join(ROOT, "cuda-mllib_b200", "libGPUALS.so"))
+    for mangled in CXX_LINKAGE.values():
+        assert mangled in syms
+    assert "doALSWithCSR" in syms and "get_gpu" in syms
+
+
+def test_reference_style_cxx_caller_links_and_runs(tmp_path):
+    """A C++ translation unit written against the reference's declarations
+    (utilities.h:36-41, als.h:96-103) links against libGPUALS.so with every
+    symbol resolved, and the drop-in's kernel-error check throws
+    thrust::system_error across the library boundary (no GPU needed)."""
+    pkg = os.path.join(ROOT, "cuda-mllib_b200")
+    exe = str(tmp_path / "cxx_caller")
+    # built for sm_100a like the library (and like the reference's JNI, which its
+    # build compiles in one nvcc command with als.cu): the inline namespace of
+    # thrust::system_error follows the target architecture
+    subprocess.run(["nvcc", "-std=c++17", "-O1", "-gencode", "arch=compute_100a,code=sm_100a",
+                    os.path.join(ROOT, "tests", "cxx_caller.cpp"),
+                    "-o", exe, "-L" + pkg, "-lGPUALS", "-Xlinker", "-rpath," + pkg],
+                   check=True, capture_output=True)
+    run = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, (run.stdout, run.stderr)
+    assert "checks 7" in run.stdout
+    assert "bounded wait timed out" in run.stderr
 
 
 def test_default_options():

@@ -120,3 +120,38 @@ def test_jni_without_gpu_returns_null():
              fk.fake_float_array(2, val.ctypes.data))
     assert not out
     assert fk.fake_live_critical() == 0
+
+
+@pytest.mark.gpu
+def test_jni_error_inside_dropin_returns_null():
+    """A CUDA-side failure raised inside doALSWithCSR (here: a rank the FP32
+    form does not take, f = 129) reaches the shim's catch block, which reports
+    it and returns null instead of letting the exception end the executor
+    process (reference CuMFJNIInterface.cpp:129-131). The CSR arrays the call
+    was given are freed on that path too."""
+    fk = _fake()
+    f, n, m = 129, 3, 2
+    th = np.arange(n * f, dtype=np.float32).reshape(n, f)
+    outer = fk.fake_object_array(1)
+    blk = fk.fake_object_array(n)
+    keep = [np.ascontiguousarray(th[i]) for i in range(n)]
+    for i, row in enumerate(keep):
+        fk.fake_set(blk, i, fk.fake_float_array(f, row.ctypes.data))
+    fk.fake_set(outer, 0, blk)
+    ptr = np.array([0, 1, 2], np.int32)
+    col = np.array([0, 2], np.int32)
+    val = np.array([4.0, 5.0], np.float32)
+    fn = A.lib.Java_org_apache_spark_ml_recommendation_CuMFJNIInterface_doALSWithCSR
+    fn.restype = ctypes.c_void_p
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.c_void_p, ctypes.c_void_p]
+    for _ in range(3):  # repeated failures leave the process and the library usable
+        out = fn(fk.fake_env(), None, m, n, f, 2, 0.05, outer,
+                 fk.fake_int_array(3, ptr.ctypes.data), fk.fake_int_array(2, col.ctypes.data),
+                 fk.fake_float_array(2, val.ctypes.data))
+        assert not out
+        assert fk.fake_live_critical() == 0
+    # a valid call afterwards still works
+    X = A.do_als_with_csr(ptr, col, val, th[:, :16].copy(), m, n, 16, 0.05)
+    assert np.isfinite(X).all()
