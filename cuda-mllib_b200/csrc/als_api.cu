@@ -160,8 +160,13 @@ struct als_model {
 namespace {
 // Warpgroup counts tried for a side, in this order: the first and last runs
 // bracket the middle one, so the steady drop of CG steps from one iteration
-// to the next cancels out of the comparison.
-constexpr int kTuneSeq[3] = {2, 3, 2};
+// to the next cancels out of the comparison. Up to f = 112 the candidates
+// are two (rows in registers) and three (rows in TMEM) warpgroups; above it,
+// two (rows in TMEM) and one (rows in registers: 255 registers a thread).
+int tune_groups(int f, int k) {
+  static constexpr int narrow[3] = {2, 3, 2}, wide[3] = {2, 1, 2};
+  return f <= 112 ? narrow[k] : wide[k];
+}
 }  // namespace
 
 extern "C" {
@@ -262,7 +267,7 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
     delete M;
     return cuda_fail(e, "als_model_create");
   }
-  if (kind != kLpNone && tc_ws_supported(f)) {
+  if (kind != kLpNone && tc_ws_takes(f, o.solver, o.cg_jacobi)) {
     // plan memory for the whole side, so a row range (fewer rows) fits it too
     for (int sd = 0; sd < 2 && e == cudaSuccess; ++sd) {
       Side &S = M->side[sd];
@@ -274,8 +279,8 @@ int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t n
       S.has_plan = e == cudaSuccess;
     }
     // the autotuner's candidates are loaded now, so no timed launch pays for it
-    for (int g = 2; g <= 3 && e == cudaSuccess && o.solver_groups == 0; ++g)
-      e = prepare_rows_tc_ws(f, kind, g);
+    for (int k = 0; k < 2 && e == cudaSuccess && o.solver_groups == 0; ++k)
+      e = prepare_rows_tc_ws(f, kind, tune_groups(f, k));
     if (e != cudaSuccess) {
       als_model_destroy(M);
       return cuda_fail(e, "als_model_create: work plan");
@@ -386,7 +391,7 @@ static cudaError_t model_half(als_model *M, int side, float lambda, cudaStream_t
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
       cudaStreamIsCapturing(st, &cs);
       if (cs == cudaStreamCaptureStatusNone && M->tev[0] && M->tev[1]) {
-        o.solver_groups = kTuneSeq[M->tune_idx[side]];
+        o.solver_groups = tune_groups(M->f, M->tune_idx[side]);
         timing = true;
       }
     }
@@ -404,7 +409,7 @@ static cudaError_t model_half(als_model *M, int side, float lambda, cudaStream_t
     M->tune_ms[side][M->tune_idx[side]++] = ms;
     if (M->tune_idx[side] == 3) {
       const float t2 = 0.5f * (M->tune_ms[side][0] + M->tune_ms[side][2]), t3 = M->tune_ms[side][1];
-      M->tuned[side] = t3 < t2 ? 3 : 2;
+      M->tuned[side] = t3 < t2 ? tune_groups(M->f, 1) : tune_groups(M->f, 0);
     }
   }
   if (M->opt.warm_start == ALS_WARM_MLP) {
@@ -1067,7 +1072,7 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
   const int kind = lp_kind_of(o.precision);
   const int ldp = kind ? tc_padded_ld(f) : 0;
   const int sms = device_sm_count();
-  const bool ws = kind != kLpNone && tc_ws_supported(f) && m > 0;
+  const bool ws = kind != kLpNone && tc_ws_takes(f, o.solver, o.cg_jacobi) && m > 0;
   // device buffers: theta (+ low-precision copy), X, widened row pointers,
   // order/queue/counters, the work plan of the warp-specialised kernel
   size_t off = 0;

@@ -55,6 +55,8 @@ struct RowsArgs {
   Counters *counters;        // optional
   float refine_tol;          // relative residual that triggers FP64 refinement
   int *error;                // sticky error word (device), may be null
+  const int *m_dev;          // optional: the number of rows, read from device memory
+                             // (m is then only an upper bound for launch sizing)
 };
 
 // A group of threads that synchronise together: the whole CTA (id 0) or a
@@ -98,7 +100,7 @@ __device__ __forceinline__ int64_t next_row(const RowsArgs &a, int *slot) {
   if (threadIdx.x == 0) *slot = (int)atomicAdd(a.queue, 1u);
   __syncthreads();
   const int64_t i = *slot;
-  if (i >= a.m) return -1;
+  if (i >= (a.m_dev ? (int64_t)*a.m_dev : a.m)) return -1;
   return a.order ? (int64_t)a.order[i] : i;
 }
 

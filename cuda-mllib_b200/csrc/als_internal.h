@@ -19,6 +19,7 @@ cudaError_t launch_rows_fp32(const RowsArgs &a, int lp_kind, int num_sms, cudaSt
 bool tc_supported(int f);
 int tc_padded_ld(int f);  // row stride (elements) of the low-precision factor copy
 struct WsPlan;
+// x0: CG starting points (rows of stride a.ld_dst), or null.
 cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
                            float cg_tol, int cg_jacobi, int groups, const float *x0,
                            const WsPlan *plan, int num_sms, cudaStream_t st);
@@ -33,6 +34,7 @@ struct TcSolve {
   int jacobi;          // 1: diagonal preconditioner
   int groups;          // solver warpgroups per CTA of the warp-specialised kernel (1, 2 or 3)
   int prepare;         // 1: only load the kernel instance and set its attributes
+  uint32_t flags_or;   // status bits added to every row's word (one-CTA-per-row kernel)
 };
 
 // Work list of the warp-specialised kernel, planned on the host per side:
@@ -60,6 +62,11 @@ struct WsPlan {
   int src_rows = 0;                    // rows of the source factor matrix (gather bounds)
   float *chol = nullptr;               // [ctas][3][kCholFloats] fallback Cholesky tiles
   int ctas = 0;                        // CTAs the scratch covers: a launch uses at most this many
+  // rows of ranks f > 112 that CG did not finish, for the post-pass of the
+  // one-CTA-per-row kernel: the rows, their count and the post-pass queue head
+  int *fb_rows = nullptr;
+  int *fb_count = nullptr;             // fb_count[0] rows, fb_count[1] queue head
+  int64_t rows = 0;                    // rows the plan covers
 };
 
 // Planning of a side's rows [begin, begin + count) on the device (no host
@@ -74,9 +81,12 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
                     int src_rows, void *mem, size_t mem_bytes, WsPlan *plan, int *error,
                     cudaStream_t st);
 
-// Warp-specialised tensor-core kernel (f in [16, 112]); launch_rows_tc
-// dispatches to it when a plan is given.
+// Warp-specialised tensor-core kernel (f in [16, 128]); launch_rows_tc
+// dispatches to it when a plan is given and tc_ws_takes holds: every rank up
+// to 112, and above that CG without the Jacobi preconditioner (its rows that
+// CG does not finish go to a post-pass of the one-CTA-per-row kernel).
 bool tc_ws_supported(int f);
+bool tc_ws_takes(int f, int solver, int jacobi);
 cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
                               const WsPlan &plan, int num_sms, cudaStream_t st);
 int tc_ws_np(int f);

@@ -384,7 +384,7 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
       a.dst[u * a.ld_dst + m] = xm;
       if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[u * a.ld_dst_lp + m] = LP(xm);
     }
-    if (a.row_flags && tid == 0) a.row_flags[u] = flags;
+    if (a.row_flags && tid == 0) a.row_flags[u] = flags | sv.flags_or;
     // the next row's gather overwrites S (the stages): make sure all reads are done
     __syncthreads();
   }
@@ -452,19 +452,39 @@ cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_ma
   if (a.ld_src != tc_padded_ld(a.f) || !a.error) return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
   TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst, cg_jacobi,
-             groups >= 1 && groups <= 3 ? groups : 2, 0};
-  if (plan && tc_ws_supported(a.f)) return launch_rows_tc_ws(a, lp_kind, sv, *plan, num_sms, st);
-  const int f = a.f, np = tc_geom(f).np;
+             groups >= 1 && groups <= 3 ? groups : 2, 0, 0u};
+  RowsArgs ap = a;
+  if (plan && tc_ws_takes(a.f, solver, cg_jacobi)) {
+    const bool post = a.f > 112;
+    if (post) {
+      if (!plan->fb_rows || !plan->fb_count) return cudaErrorInvalidValue;
+      cudaError_t e = cudaMemsetAsync(plan->fb_count, 0, 2 * sizeof(int), st);
+      if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = launch_rows_tc_ws(a, lp_kind, sv, *plan, num_sms, st);
+    if (e != cudaSuccess || !post || sv.prepare) return e;
+    // The post-pass: the rows CG did not finish (listed by the warp-specialised
+    // kernel, count in device memory), solved here by Cholesky with
+    // FP64-residual refinement; their status words carry the CG fallback bit.
+    ap.order = plan->fb_rows;
+    ap.m_dev = plan->fb_count;
+    ap.queue = reinterpret_cast<unsigned *>(plan->fb_count + 1);
+    ap.m = plan->rows > 0 ? plan->rows : a.m;
+    sv.solver = 0;
+    sv.flags_or = kRowCgFallback;
+  }
+  const RowsArgs &a2 = ap;
+  const int f = a2.f, np = tc_geom(f).np;
   // (FP, NP): FP >= f is the Cholesky tile extent, NP = roundup16(f + 1) the MMA N
-  if (np == 32) return launch_tc_np<32, 32>(a, lp_kind, sv, num_sms, st);
-  if (np == 48) return launch_tc_np<64, 48>(a, lp_kind, sv, num_sms, st);
-  if (np == 64) return launch_tc_np<64, 64>(a, lp_kind, sv, num_sms, st);
-  if (np == 80) return launch_tc_np<104, 80>(a, lp_kind, sv, num_sms, st);
-  if (np == 96) return launch_tc_np<104, 96>(a, lp_kind, sv, num_sms, st);
-  if (np == 112 && f <= 104) return launch_tc_np<104, 112>(a, lp_kind, sv, num_sms, st);
-  if (np == 112) return launch_tc_np<128, 112>(a, lp_kind, sv, num_sms, st);
-  if (np == 128) return launch_tc_np<128, 128>(a, lp_kind, sv, num_sms, st);
-  if (np == 144) return launch_tc_np<128, 144>(a, lp_kind, sv, num_sms, st);
+  if (np == 32) return launch_tc_np<32, 32>(a2, lp_kind, sv, num_sms, st);
+  if (np == 48) return launch_tc_np<64, 48>(a2, lp_kind, sv, num_sms, st);
+  if (np == 64) return launch_tc_np<64, 64>(a2, lp_kind, sv, num_sms, st);
+  if (np == 80) return launch_tc_np<104, 80>(a2, lp_kind, sv, num_sms, st);
+  if (np == 96) return launch_tc_np<104, 96>(a2, lp_kind, sv, num_sms, st);
+  if (np == 112 && f <= 104) return launch_tc_np<104, 112>(a2, lp_kind, sv, num_sms, st);
+  if (np == 112) return launch_tc_np<128, 112>(a2, lp_kind, sv, num_sms, st);
+  if (np == 128) return launch_tc_np<128, 128>(a2, lp_kind, sv, num_sms, st);
+  if (np == 144) return launch_tc_np<128, 144>(a2, lp_kind, sv, num_sms, st);
   return cudaErrorNotSupported;
 }
 

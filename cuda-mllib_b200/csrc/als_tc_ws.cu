@@ -59,9 +59,23 @@ template <int NG> __host__ __device__ constexpr int mma_warp() { return 4 * NG +
 constexpr int NS = 6;                             // shared-memory stages
 constexpr int KS = 64;                            // ratings per stage
 constexpr int kAtom = (KS / 8) * 1024;            // one 64-element MN atom of a stage
-constexpr int kStageBytes = 2 * kAtom;            // tile columns 0-63 and 64-127
-constexpr int kAcc = 4;                           // TMEM accumulators (row n -> n mod 4)
+constexpr int kMaxAcc = 4;                        // TMEM accumulators at most
 constexpr int kMaxGroups = 3;                     // solver warpgroups per CTA at most
+// Shape of an instance by its Cholesky tile extent FP (f <= FP): up to f = 112
+// a stage holds tile columns 0-127 (two 64-column atoms: the factor row and
+// the rating column c_r = ld <= 120) and four 128-column accumulators fill
+// TMEM. Above (f <= 128, ld <= 136) a stage needs a third atom and the MMA's N
+// reaches 144, so TMEM holds three accumulators of 160 columns; a 128-wide
+// Cholesky tile would need 136 tiles for 128 threads, so rows CG cannot finish
+// are handed to a post-pass of the one-CTA-per-row kernel.
+template <int FP> struct Dims {
+  static constexpr bool kWide = FP > 112;
+  static constexpr int kAtoms = kWide ? 3 : 2;
+  static constexpr int kStageBytes = kAtoms * kAtom;
+  static constexpr int kAcc = kWide ? 3 : 4;          // row n -> accumulator n mod kAcc
+  static constexpr int kBufCols = kWide ? 160 : 128;  // TMEM columns per accumulator
+  static constexpr bool kChol = !kWide;               // the in-kernel Cholesky fallback
+};
 // Row hand-over slots: kGroupSlots per solver warpgroup. Row n goes to group
 // n mod NG, the k-th row of a group (k = n / NG) to its slot k mod
 // kGroupSlots, as that slot's (k / kGroupSlots)-th barrier phase. An mbarrier
@@ -69,10 +83,13 @@ constexpr int kMaxGroups = 3;                     // solver warpgroups per CTA a
 // wait may name a phase two ahead of its barrier's:
 //  - a group waits only on its own slots, in its own order;
 //  - a producer posting row r waits for the slot's previous row, r - 8 NG,
-//    to have been taken; when it can post row r, the MMA has taken stage
-//    (first stage of r) - NS and so started row >= r - NS, hence rows up to
-//    r - NS - kAcc = r - 10 are solved and their successors' rows taken, and
-//    r - 16 NG (two slot uses back) is long taken.
+//    to have been taken. When it posts row r it has finished its previous
+//    stage, (first stage of r) - P with P producers, whose slot wait means
+//    the MMA has issued stage (first stage of r) - P - NS and so acquired
+//    the accumulator of its row R' >= r - P - NS; every row up to
+//    R' - kAcc >= r - P - NS - kAcc >= r - 13 has then handed its
+//    accumulator back, so it has been taken, and r - 16 NG (two slot uses
+//    back) is among them.
 constexpr int kGroupSlots = 8;
 constexpr int kRowSlots = kGroupSlots * kMaxGroups;
 template <int NG> __host__ __device__ constexpr int row_slot(long long n) {
@@ -81,8 +98,7 @@ template <int NG> __host__ __device__ constexpr int row_slot(long long n) {
 template <int NG> __host__ __device__ constexpr unsigned row_parity(long long n) {
   return (unsigned)((n / NG) / kGroupSlots) & 1u;
 }
-constexpr int kBufCols = 128;                     // TMEM columns per accumulator
-constexpr int kTmemCols = kAcc * kBufCols;        // all 512 columns
+constexpr int kTmemCols = 512;                    // allocated: all of TMEM
 constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
 constexpr int DI = 8;                             // index-ring slots (stages fetched ahead + 1)
 constexpr int kRingSlot = 8 * KS + 48;            // column indices, ratings, three int4 of header
@@ -91,7 +107,7 @@ static_assert(NS % kProducers == 0, "a stage slot always belongs to the same pro
 }  // namespace ws
 
 struct WsGeom {
-  int nj;  // 16-byte pieces per factor row (ld_src / 8, at most 16)
+  int nj;  // 16-byte pieces per factor row (ld_src / 8, at most 17)
 };
 
 // Per solver warpgroup: the fallback Cholesky's tile when shared memory has
@@ -100,23 +116,28 @@ struct WsGeom {
 template <int FP, int NP, int NG, bool SIN>
 struct WsLayoutT {
   static constexpr int LDS = FP + 1;
-  static_assert((size_t)FP * LDS <= (size_t)kCholFloats, "Cholesky tile fits its scratch");
-  static constexpr bool kSInSmem = SIN;
-  static constexpr size_t kS = SIN ? (size_t)FP * LDS * 4 : 0;
+  static constexpr bool kChol = ws::Dims<FP>::kChol;  // wide instances have no tile
+  static_assert(!kChol || (size_t)FP * LDS <= (size_t)kCholFloats, "Cholesky tile fits its scratch");
+  static constexpr bool kSInSmem = SIN && kChol;
+  static constexpr size_t kS = kSInSmem ? (size_t)FP * LDS * 4 : 0;
   static constexpr size_t oDg = kS, oBv = oDg + FP * 4, oXv = oBv + FP * 4, oTmp = oXv + FP * 4;
   static constexpr size_t oPs = (oTmp + FP * 4 + 15) / 16 * 16;
-  static constexpr int kPs = 128;  // CG broadcast vector: one entry per thread of the warpgroup
-  static_assert(NP <= kPs, "the broadcast vector covers every accumulator column");
+  // CG broadcast vectors: two barrier phases x two vectors x one entry per
+  // thread of the warpgroup (the TMEM-resident solver uses the first 128)
+  static constexpr int kPs = 512;
+  static_assert(NP <= 128, "the broadcast vector covers every accumulator column");
   static constexpr size_t oRed = oPs + kPs * 4;
-  static constexpr size_t oRd = (oRed + 80 * 4 + 7) / 8 * 8;  // 8 CG + 64 refinement + pad
+  // 64 CG partial sums (two barrier phases of 32) + 64 refinement
+  static constexpr size_t oRd = (oRed + 128 * 4 + 7) / 8 * 8;
   static constexpr size_t oMisc = oRd + (size_t)FP * 8;
-  static constexpr size_t kSolver = (oMisc + 16 + 127) / 128 * 128;
-  static constexpr size_t oSolver = (size_t)ws::NS * ws::kStageBytes;
+  static constexpr size_t oCnt = oMisc + 16;  // six 64-bit counters of the group
+  static constexpr size_t kSolver = (oCnt + 48 + 127) / 128 * 128;
+  static constexpr size_t oSolver = (size_t)ws::NS * ws::Dims<FP>::kStageBytes;
   static constexpr size_t oCtrl = oSolver + NG * kSolver;
   // full, empty per stage; acc_full, acc_empty per accumulator (row n uses
   // accumulator n mod kAcc); row_full, row_empty per row slot; drain; one
   // spare (16-byte multiple)
-  static constexpr size_t kBars = 8 * (2 * ws::NS + 2 * ws::kAcc + 2 * ws::kRowSlots + 2);
+  static constexpr size_t kBars = 8 * (2 * ws::NS + 2 * ws::kMaxAcc + 2 * ws::kRowSlots + 2);
   static constexpr size_t kCtrl = kBars + 16 * (ws::NS + ws::kRowSlots) + 16;
   static constexpr size_t oRing = oCtrl + kCtrl;  // 16-byte aligned
   static constexpr size_t kTotal = 1024 + oRing + (size_t)ws::kProducers * ws::DI * ws::kRingSlot;
@@ -166,8 +187,10 @@ struct ItemBatch {
 
 __device__ __forceinline__ ItemBatch load_batch(const WsPlan &p, long long bi, int lane) {
   const long long i = blockIdx.x + (bi * 32 + lane) * (long long)gridDim.x;
+  // the item count of a plan built on the device is read from device memory
+  const int nitems = p.nitems_dev ? *p.nitems_dev : p.nitems;
   ItemBatch b;
-  if (i < p.nitems) {
+  if (i < nitems) {
     const int4 *q = reinterpret_cast<const int4 *>(p.items + i);
     b.lo = q[0];
     b.hi = q[1];
@@ -298,6 +321,23 @@ struct FetchCursor {
 __device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &plan, int nj,
                                              const int *cols, int kc, int krows, uint32_t sa,
                                              int lane) {
+  if (nj > 16) {
+    // piece 16 (tile columns 128-135, atom 2, 16-byte chunk 0 xor (k mod 8)) of
+    // rows lane and lane + 32, for ranks f > 120
+    const char *src16 = reinterpret_cast<const char *>(a.src) + 16 * 16;
+    const unsigned row_bytes = (unsigned)a.ld_src * 2u, last = (unsigned)plan.src_rows - 1u;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = lane + 32 * h;
+      if (k < krows) {
+        const bool in = k < kc;
+        const unsigned c = in ? min((unsigned)cols[k], last) : 0u;
+        const uint32_t dst = sa + 2u * ws::kAtom + (uint32_t)((k >> 3) * 1024 + (k & 7) * 128) +
+                             ((uint32_t)(k & 7) << 4);
+        cp_async16_zfill(dst, in ? src16 + (size_t)c * row_bytes : src16, in ? 16u : 0u);
+      }
+    }
+  }
   const int j = lane & 15, k0 = (lane >> 4) * 32;
   if (j >= nj || k0 >= krows) return;
   int ci[32];
@@ -342,7 +382,7 @@ __device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &pl
 // coordination beyond those barriers.
 // The producer that owns the stage just past the last one writes the end
 // markers.
-template <typename LP, int NG>
+template <int FP, typename LP, int NG>
 __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &g,
                            const WsCtrl &c, unsigned char *stages, unsigned char *ring, int k,
                            unsigned long long &n_empty_rows) {
@@ -381,7 +421,7 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     }
     // every stage of row h2.x accumulates into accumulator h2.x mod kAcc, whichever
     // producer took the row's first stage
-    const int acc = h2.x & (ws::kAcc - 1);
+    const int acc = (int)((unsigned)h2.x % (unsigned)ws::Dims<FP>::kAcc);
     if (first) {
       // the row's first stage also hands row h2.x to its solver group
       const int r = h2.x, rs2 = ws::row_slot<NG>(r);
@@ -400,7 +440,7 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     if (st >= ws::NS)
       okw = tc::mbar_wait_or_abort(&c.empty[slot], (unsigned)((st / ws::NS) - 1) & 1u, c.misc + 1);
     if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
-    const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
+    const uint32_t sa = st0 + (uint32_t)slot * ws::Dims<FP>::kStageBytes;
     if (lane == 0) c.stage_info[slot] = make_int4(acc, krows / 16, first, last);
     gather_stage(a, plan, g.nj, reinterpret_cast<const int *>(rs), kc, krows, sa, lane);
     // r_uk (0 past kc) into tile column c_r = 8 nj: atom c_r / 64, 16-byte
@@ -443,6 +483,7 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
 // ---------------------------------------------------------------------------
 // MMA issuer (one thread)
 // ---------------------------------------------------------------------------
+template <int FP>
 __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages, uint32_t tmem,
                        uint32_t idesc) {
   const uint32_t lbo = (ws::KS / 8) * 1024, sbo = 1024;
@@ -471,10 +512,10 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
       acc_used |= 1u << b;
     }
     tc::tc_fence_after();
-    const uint32_t sa = st0 + (uint32_t)slot * ws::kStageBytes;
+    const uint32_t sa = st0 + (uint32_t)slot * ws::Dims<FP>::kStageBytes;
     for (int kk = 0; kk < kmma; ++kk) {
       const uint64_t desc = tc::make_desc(sa + kk * 2 * sbo, lbo, sbo);
-      tc::mma_f16(tmem + (uint32_t)b * ws::kBufCols, desc, desc, idesc,
+      tc::mma_f16(tmem + (uint32_t)b * ws::Dims<FP>::kBufCols, desc, desc, idesc,
                   (first && kk == 0) ? 0u : 1u);
     }
     tc::mma_commit(&c.empty[slot]);
@@ -489,6 +530,54 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
 // ---------------------------------------------------------------------------
 // solver warpgroup
 // ---------------------------------------------------------------------------
+// Register-tile Cholesky of the system in S (identity padding beyond f),
+// lambda * n_u added on the diagonal, triangular solves and the FP64-residual
+// refinement; the solution lands in xv. Returns 0, 1 (not SPD: xv = 0) or 2
+// (refined). Kept out of line so the CG loop is register-allocated on its own.
+template <int FP>
+__device__ __noinline__ int ws_cholesky(float *S, float *dg, float *bv, float *xv, float *tmp,
+                                        double *rd, float *red, int *bad, int f, float reg,
+                                        float refine_tol, const Bar &B) {
+  constexpr int LDS = FP + 1, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
+  const int lt = B.tid;
+  int ti = 0, tj = 0;
+  const bool owner = lt < NTILES;
+  if (owner) tile_of(lt, ti, tj);
+  float acc[8][8];
+  if (owner) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) {
+        const int i = 8 * ti + r, j = 8 * tj + cc;
+        float v = S[i * LDS + j];
+        if (i == j && i < f) v += reg;
+        acc[r][cc] = v;
+      }
+  }
+  B.sync();
+  if (owner && ti == tj) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = 8 * ti + r;
+      dg[i] = acc[r][r];
+      xv[i] = bv[i];
+    }
+  }
+  const bool okc = tile_cholesky<FP, LDS, 128>(acc, ti, tj, owner, S, bad, B);
+  if (!okc) {
+    for (int i = lt; i < f; i += 128) xv[i] = 0.f;
+    B.sync();
+    return 1;
+  }
+  bool refined = false;
+  solve_and_refine<FP, LDS, 128>(S, dg, bv, xv, rd, tmp, f, refine_tol, &refined, red, B);
+  return refined ? 2 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// solver warpgroup, ranks up to 112 (system kept in TMEM)
+// ---------------------------------------------------------------------------
 // Row m of (D + diag I) times the broadcast vector v, with row m of D read
 // from TMEM (lane m of accumulator tA) 32 columns at a time (64 per wait
 // measured slower): the system stays
@@ -496,7 +585,7 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
 // independent FMA chains, carried two to an instruction by the packed FP32
 // FMA of sm_100.
 template <int NP>
-__device__ __forceinline__ float matvec_tmem(uint32_t tA, const float *v, float diag, float vm) {
+__device__ __forceinline__ float matvec_tmem_np(uint32_t tA, const float *v, float diag, float vm) {
   float2 q01 = make_float2(diag * vm, 0.f), q23 = make_float2(0.f, 0.f);
 #pragma unroll
   for (int c0 = 0; c0 < NP; c0 += 32) {
@@ -576,51 +665,6 @@ __device__ __forceinline__ float4 group_sum4(float4 v, float *red, int &slot, co
   return t;
 }
 
-// Register-tile Cholesky of the system in S (identity padding beyond f),
-// lambda * n_u added on the diagonal, triangular solves and the FP64-residual
-// refinement; the solution lands in xv. Returns 0, 1 (not SPD: xv = 0) or 2
-// (refined). Kept out of line so the CG loop is register-allocated on its own.
-template <int FP>
-__device__ __noinline__ int ws_cholesky(float *S, float *dg, float *bv, float *xv, float *tmp,
-                                        double *rd, float *red, int *bad, int f, float reg,
-                                        float refine_tol, const Bar &B) {
-  constexpr int LDS = FP + 1, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
-  const int lt = B.tid;
-  int ti = 0, tj = 0;
-  const bool owner = lt < NTILES;
-  if (owner) tile_of(lt, ti, tj);
-  float acc[8][8];
-  if (owner) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-      for (int cc = 0; cc < 8; ++cc) {
-        const int i = 8 * ti + r, j = 8 * tj + cc;
-        float v = S[i * LDS + j];
-        if (i == j && i < f) v += reg;
-        acc[r][cc] = v;
-      }
-  }
-  B.sync();
-  if (owner && ti == tj) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = 8 * ti + r;
-      dg[i] = acc[r][r];
-      xv[i] = bv[i];
-    }
-  }
-  const bool okc = tile_cholesky<FP, LDS, 128>(acc, ti, tj, owner, S, bad, B);
-  if (!okc) {
-    for (int i = lt; i < f; i += 128) xv[i] = 0.f;
-    B.sync();
-    return 1;
-  }
-  bool refined = false;
-  solve_and_refine<FP, LDS, 128>(S, dg, bv, xv, rd, tmp, f, refine_tol, &refined, red, B);
-  return refined ? 2 : 0;
-}
-
 // Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA. Row n
 // arrives in row slot row_slot<NG>(n) and accumulator n mod kAcc (the
 // (n / kAcc)-th phase of its barriers); the group keeps the accumulator until the row is solved:
@@ -631,7 +675,8 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   using L = WsLayout<FP, NP, NG>;
   constexpr int LDS = L::LDS, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
   static_assert(NTILES <= 128, "one warpgroup holds at most 128 Cholesky tiles");
-  static_assert(NP <= ws::kBufCols, "the system fits one accumulator");
+  static_assert(NP <= ws::Dims<FP>::kBufCols, "the system fits one accumulator");
+  static_assert(!ws::Dims<FP>::kWide, "ranks up to 112");
   const int lt = threadIdx.x & 127, wl = (threadIdx.x >> 5) & 3;
   const Bar B{1 + wg, 128, lt};
   float *S = L::kSInSmem ? reinterpret_cast<float *>(mem)
@@ -651,9 +696,9 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   const uint32_t bcol = (uint32_t)(a.ld_src & ~15);
   const int bq = a.ld_src & 15;
   for (long long n = wg;; n += NG) {
-    const int rb = ws::row_slot<NG>(n), ab = (int)(n & (ws::kAcc - 1));
-    const unsigned par = (unsigned)(n / ws::kAcc) & 1u;
-    const uint32_t tA = tlane + (uint32_t)ab * ws::kBufCols;
+    const int rb = ws::row_slot<NG>(n), ab = (int)(n & (ws::Dims<FP>::kAcc - 1));
+    const unsigned par = (unsigned)(n / ws::Dims<FP>::kAcc) & 1u;
+    const uint32_t tA = tlane + (uint32_t)ab * ws::Dims<FP>::kBufCols;
     bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], ws::row_parity<NG>(n), c.misc + 1);
     if (!B.all(ok)) { ws_abort(a, c); break; }
     const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[rb]);
@@ -760,7 +805,7 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
         // the start is never worse than zero in that norm.
         ps[m] = x;
         B.sync();
-        float q0 = matvec_tmem<NP>(tA, ps, reg, x);
+        float q0 = matvec_tmem_np<NP>(tA, ps, reg, x);
         if (!live) q0 = 0.f;
         const float2 xs = group_sum2(x * bm, x * q0, red, rslot, B);
         float sc = xs.x / xs.y;
@@ -784,7 +829,7 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       int it = 0;
       float p = 0.f, w = 0.f, beta = 0.f;
       while (!conv && it < sv.cg_max_steps) {
-        float az = matvec_tmem<NP>(tA, ps, reg, z);
+        float az = matvec_tmem_np<NP>(tA, ps, reg, z);
         if (!live) az = 0.f;
         p = fmaf(beta, p, z);
         w = fmaf(beta, w, az);
@@ -859,6 +904,525 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   }
 }
 
+// ---------------------------------------------------------------------------
+// solver warpgroup, ranks above 112
+// ---------------------------------------------------------------------------
+// Row m of (D + diag I) times the broadcast vector v: four independent FMA
+// chains over the columns in steps of eight, two lanes each (packed FP32
+// FMA). matvec_reg takes row m of D from registers, matvec_tmem from TMEM lane
+// m of accumulator tA; both do the same operations in the same order, so the
+// two placements of the system give the same bits.
+__device__ __forceinline__ void mv8(float2 (&q)[4], const float *A8, const float *v8) {
+  const float4 a4 = *reinterpret_cast<const float4 *>(v8);
+  const float4 b4 = *reinterpret_cast<const float4 *>(v8 + 4);
+  q[0] = __ffma2_rn(make_float2(A8[0], A8[1]), make_float2(a4.x, a4.y), q[0]);
+  q[1] = __ffma2_rn(make_float2(A8[2], A8[3]), make_float2(a4.z, a4.w), q[1]);
+  q[2] = __ffma2_rn(make_float2(A8[4], A8[5]), make_float2(b4.x, b4.y), q[2]);
+  q[3] = __ffma2_rn(make_float2(A8[6], A8[7]), make_float2(b4.z, b4.w), q[3]);
+}
+__device__ __forceinline__ float mv_total(const float2 (&q)[4]) {
+  return ((q[0].x + q[0].y) + (q[1].x + q[1].y)) + ((q[2].x + q[2].y) + (q[3].x + q[3].y));
+}
+
+template <int KA>
+__device__ __forceinline__ float matvec_reg(const float (&A)[KA], const float *v, float diag,
+                                            float vm) {
+  static_assert(KA % 8 == 0, "eight columns per step");
+  float2 q[4] = {make_float2(diag * vm, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                 make_float2(0.f, 0.f)};
+#pragma unroll
+  for (int k = 0; k < KA; k += 8) {
+    // A compiler-only barrier every 32 columns keeps the vector's loads from
+    // being hoisted all at once beside the row.
+    if (k % 32 == 0 && k > 0) asm volatile("" ::: "memory");
+    mv8(q, A + k, v + k);
+  }
+  return mv_total(q);
+}
+
+template <int KA>
+__device__ __forceinline__ float matvec_tmem(uint32_t tA, const float *v, float diag, float vm) {
+  static_assert(KA % 8 == 0, "eight columns per step");
+  float2 q[4] = {make_float2(diag * vm, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                 make_float2(0.f, 0.f)};
+#pragma unroll
+  for (int c0 = 0; c0 < KA; c0 += 32) {
+    float d[32];
+    if (KA - c0 > 16) {
+      tc::tmem_ld32(tA + (uint32_t)c0, d);
+    } else {
+      float h[16];
+      tc::tmem_ld16(tA + (uint32_t)c0, h);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) d[k] = h[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 32; k += 8)
+      if (c0 + k < KA) mv8(q, d + k, v + c0 + k);
+  }
+  return mv_total(q);
+}
+
+// The first half of a four-value warpgroup sum, split from its barrier so the
+// barrier can also publish a broadcast vector: the warp's four partial sums
+// (lane quarters split the shuffle tree: six shuffles for four sums) go to
+// r[4 w .. 4 w + 3]. After the barrier, group_read4(r) gives the totals.
+__device__ __forceinline__ void group_partial4(float4 v, float *r, int tid) {
+  const int lane = tid & 31;
+  const bool h16 = lane & 16, h8 = lane & 8;
+  float x0 = h16 ? v.z : v.x, x1 = h16 ? v.w : v.y;
+  x0 += __shfl_xor_sync(0xffffffffu, h16 ? v.x : v.z, 16);
+  x1 += __shfl_xor_sync(0xffffffffu, h16 ? v.y : v.w, 16);
+  float x = h8 ? x1 : x0;
+  x += __shfl_xor_sync(0xffffffffu, h8 ? x0 : x1, 8);
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  // lane 0: v.x, lane 8: v.y, lane 16: v.z, lane 24: v.w
+  if ((lane & 7) == 0) r[(tid >> 5) * 4 + (lane >> 3)] = x;
+}
+// One and two values: the same split, with the shuffle trees of one value
+// (five shuffles) and of two (lanes 0-15 keep a, 16-31 b: five shuffles).
+__device__ __forceinline__ void group_partial1(float a, float *r, int tid) {
+  a = warp_sum(a);
+  if ((tid & 31) == 0) r[tid >> 5] = a;
+}
+__device__ __forceinline__ float group_read1(const float *r) {
+  const float4 q = *reinterpret_cast<const float4 *>(r);
+  return (q.x + q.y) + (q.z + q.w);
+}
+__device__ __forceinline__ void group_partial2(float a, float b, float *r, int tid) {
+  const int lane = tid & 31;
+  const bool hi = lane & 16;
+  float x = hi ? b : a;
+  x += __shfl_xor_sync(0xffffffffu, hi ? a : b, 16);
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  if ((lane & 15) == 0) r[(tid >> 5) * 2 + (lane >> 4)] = x;
+}
+__device__ __forceinline__ float2 group_read2(const float *r) {
+  float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const float2 q = reinterpret_cast<const float2 *>(r)[w];
+    t.x += q.x;
+    t.y += q.y;
+  }
+  return t;
+}
+__device__ __forceinline__ float4 group_read4(const float *r) {
+  float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const float4 q = reinterpret_cast<const float4 *>(r)[w];
+    t.x += q.x; t.y += q.y; t.z += q.z; t.w += q.w;
+  }
+  return t;
+}
+
+// Columns [0, KA) of this thread's TMEM lane of accumulator tA into A (KA a
+// multiple of 8, at most 128): every load issued before one wait. Each load
+// fills a fixed-size array and all indices are constants, so everything
+// stays in registers.
+template <int KA>
+__device__ __forceinline__ void tmem_row_to_regs(uint32_t tA, float (&A)[KA]) {
+  static_assert(KA % 8 == 0 && KA <= 128, "row held in at most four 32-column loads");
+  uint32_t r[4][32], t[16];
+  constexpr int n32 = KA / 32, rem = KA - 32 * n32;  // rem in {0, 8, 16, 24}
+#pragma unroll
+  for (int b = 0; b < n32; ++b) tc::tmem_ld32_nowait(tA + 32 * b, r[b]);
+  if constexpr (rem > 16) tc::tmem_ld32_nowait(tA + 32 * n32, r[n32 < 4 ? n32 : 0]);
+  else if constexpr (rem > 0) tc::tmem_ld16_nowait(tA + 32 * n32, t);
+  tc::tmem_wait_ld();
+#pragma unroll
+  for (int k = 0; k < KA; ++k) {
+    uint32_t v = (k / 32 < n32 || rem > 16) ? r[k / 32][k % 32] : t[k % 32 < 16 ? k % 32 : 0];
+    tc::tmem_launder(v);
+    A[k] = __uint_as_float(v);
+  }
+}
+
+// Where a solver warpgroup keeps the row's system while it solves it: in
+// registers (thread m holds row m of A_u; the accumulator goes back to the MMA
+// thread as soon as the row is copied out, so the next rows' hermitians
+// accumulate while this one is solved), or in its TMEM accumulator (kept for
+// the whole solve; for builds whose registers cannot hold a row).
+template <int KA, bool REG>
+struct RowSystem;
+template <int KA>
+struct RowSystem<KA, true> {
+  float A[KA];
+  __device__ __forceinline__ float mv(const float *v, float diag, float vm) const {
+    return matvec_reg<KA>(A, v, diag, vm);
+  }
+  __device__ __forceinline__ void load(uint32_t tA) { tmem_row_to_regs<KA>(tA, A); }
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int k = 0; k < KA; ++k) A[k] = 0.f;
+  }
+  // the row into a row of the Cholesky tile (columns [0, KA)) when `write`
+  __device__ __forceinline__ void store(float *Sr, bool write) const {
+    if (!write) return;
+#pragma unroll
+    for (int k = 0; k < KA; ++k) Sr[k] = A[k];
+  }
+  // add a partial sum (a split row's chunk slot) into the row
+  __device__ __forceinline__ void add(const float *Q) {
+#pragma unroll
+    for (int c0 = 0; c0 < KA; c0 += 4) {
+      const float4 w4 = __ldcg(reinterpret_cast<const float4 *>(Q + c0));
+      A[c0] += w4.x; A[c0 + 1] += w4.y; A[c0 + 2] += w4.z; A[c0 + 3] += w4.w;
+    }
+  }
+  __device__ __forceinline__ void save_partial(float *P, bool live, uint32_t) const {
+#pragma unroll
+    for (int c0 = 0; c0 < KA; c0 += 4)
+      __stcg(reinterpret_cast<float4 *>(P + c0),
+             live ? make_float4(A[c0], A[c0 + 1], A[c0 + 2], A[c0 + 3]) : make_float4(0.f, 0.f, 0.f, 0.f));
+  }
+};
+template <int KA>
+struct RowSystem<KA, false> {
+  uint32_t tA;
+  __device__ __forceinline__ float mv(const float *v, float diag, float vm) const {
+    return matvec_tmem<KA>(tA, v, diag, vm);
+  }
+  __device__ __forceinline__ void load(uint32_t t) { tA = t; }
+  // Every thread of the warp must call this (the TMEM loads are
+  // warp-collective); only threads with `write` store.
+  __device__ __forceinline__ void store(float *Sr, bool write) const {
+#pragma unroll
+    for (int c0 = 0; c0 < KA; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(tA + (uint32_t)c0, v);
+      if (write) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          if (c0 + q < KA) Sr[c0 + q] = v[q];
+      }
+    }
+  }
+  __device__ __forceinline__ void save_partial(float *P, bool live, uint32_t) const {
+#pragma unroll
+    for (int c0 = 0; c0 < KA; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(tA + (uint32_t)c0, v);
+#pragma unroll
+      for (int q = 0; q < 16; q += 4)
+        if (c0 + q < KA)
+          __stcg(reinterpret_cast<float4 *>(P + c0 + q),
+                 live ? make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]) : make_float4(0.f, 0.f, 0.f, 0.f));
+    }
+  }
+  // the sum of a split row's chunk slots into the accumulator, in chunk order
+  __device__ __forceinline__ void sum_partials(const float *partial, int base, int nch, int m,
+                                               int part_ld) {
+#pragma unroll
+    for (int c0 = 0; c0 < KA; c0 += 16) {
+      float v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = 0.f;
+      for (int ch = 0; ch < nch; ++ch) {
+        const float *Q = partial + ((size_t)(base + ch) * 128 + m) * part_ld + c0;
+#pragma unroll
+        for (int q = 0; q < 16; q += 4) {
+          if (c0 + q < KA) {
+            const float4 w4 = __ldcg(reinterpret_cast<const float4 *>(Q + q));
+            v[q] += w4.x; v[q + 1] += w4.y; v[q + 2] += w4.z; v[q + 3] += w4.w;
+          }
+        }
+      }
+      tc::tmem_st16(tA + (uint32_t)c0, v);
+    }
+  }
+};
+
+// Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA. Row n
+// arrives in row slot row_slot<NG>(n) and accumulator n mod kAcc (the
+// (n / kAcc)-th phase of its barriers). CG (optionally Jacobi-preconditioned)
+// from the warm start scaled optimally along itself, to relative residual
+// cg_tol in at most cg_max_steps steps; a reduction is written as partial sums
+// before its barrier and read after it, and the barriers that publish the
+// warm start and the search direction are the ones the group needs anyway (the
+// accumulator vote, and the reduction of r.z and r.r). Rows CG does not
+// finish, or along whose search direction A is not positive, are solved by the
+// register-tile Cholesky with FP64-residual refinement; so is every row when
+// sv.solver == 0.
+template <int FP, int NP, typename LP, int NG, bool REG>
+__device__ void ws_solve_wide(const RowsArgs &a, const WsPlan &plan, const TcSolve &sv,
+                         const WsCtrl &c, unsigned char *mem, uint32_t tmem, int wg) {
+  using L = WsLayout<FP, NP, NG>;
+  constexpr int LDS = L::LDS, NTILES = (FP / 8) * (FP / 8 + 1) / 2;
+  static_assert(!L::kChol || NTILES <= 128, "one warpgroup holds at most 128 Cholesky tiles");
+  using D = ws::Dims<FP>;
+  static_assert(NP <= D::kBufCols, "the system fits one accumulator");
+  // columns of the system per thread: f <= min(NP, FP); the rest of the
+  // accumulator is padding (and the b_u column)
+  constexpr int KA = NP < FP ? NP : FP;
+  const int lt = threadIdx.x & 127, wl = (threadIdx.x >> 5) & 3;
+  const Bar B{1 + wg, 128, lt};
+  float *S = L::kSInSmem ? reinterpret_cast<float *>(mem)
+                         : plan.chol + ((size_t)blockIdx.x * ws::kMaxGroups + wg) * kCholFloats;
+  float *dg = reinterpret_cast<float *>(mem + L::oDg), *bv = reinterpret_cast<float *>(mem + L::oBv);
+  float *xv = reinterpret_cast<float *>(mem + L::oXv), *tmp = reinterpret_cast<float *>(mem + L::oTmp);
+  float *pv = reinterpret_cast<float *>(mem + L::oPs), *red = reinterpret_cast<float *>(mem + L::oRed);
+  double *rd = reinterpret_cast<double *>(mem + L::oRd);
+  int *bad = reinterpret_cast<int *>(mem + L::oMisc);
+  const int f = a.f, m = lt;
+  const bool live = m < f;
+  for (int i = lt; i < L::kPs; i += 128) pv[i] = 0.f;
+  B.sync();
+  // Phase of the barriers that publish vectors or partial sums: the k-th such
+  // barrier of the group uses buffer k mod 2 (vectors pv[256 (k mod 2) ...],
+  // partials red[32 (k mod 2) ...]). A buffer is written again only two
+  // barriers later, when every thread has finished reading it.
+  int ph = 0;
+  auto vbuf = [&](int k) { return pv + (ph & 1) * 256 + k * 128; };
+  auto rbuf = [&]() { return red + (ph & 1) * 32; };
+  // counters of the group, kept by thread 0 in shared memory (not registers)
+  unsigned long long *cnt = reinterpret_cast<unsigned long long *>(mem + L::oCnt);
+  if (lt == 0)
+    for (int k = 0; k < 6; ++k) cnt[k] = 0;
+  const uint32_t tlane = tmem + ((uint32_t)(wl * 32) << 16);
+  const uint32_t bcol = (uint32_t)(a.ld_src & ~15);
+  const int bq = a.ld_src & 15;
+  const bool cg = sv.solver == 1;
+  for (long long n = wg;; n += NG) {
+    const int rb = ws::row_slot<NG>(n);
+    const int ab = (int)((unsigned long long)n % (unsigned)D::kAcc);
+    const unsigned par = (unsigned)((unsigned long long)n / (unsigned)D::kAcc) & 1u;
+    const uint32_t tA = tlane + (uint32_t)ab * D::kBufCols;
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], ws::row_parity<NG>(n), c.misc + 1);
+    int4 info = make_int4(-1, 0, 0, 0);
+    if (ok) {
+      const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[rb]);
+      info = make_int4(vi[0], vi[1], vi[2], vi[3]);
+    }
+    // every thread has read the slot once all have passed this barrier
+    if (!B.all(ok)) { ws_abort(a, c); break; }
+    if (lt == 0) tc::mbar_arrive(&c.row_empty[rb]);
+    if (info.x < 0) break;
+    const int64_t u = info.x;
+    const float reg = a.lambda * (float)info.y;
+    // the warm start's load overlaps the wait for the accumulator, and (for a
+    // whole row) it is published with the accumulator vote
+    float x = (live && sv.x0 && info.z < 0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
+    if (!isfinite(x)) x = 0.f;
+    if (cg && info.z < 0) vbuf(0)[m] = x;
+    ok = tc::mbar_wait_or_abort(&c.acc_full[ab], par, c.misc + 1);
+    if (!B.all(ok)) { ws_abort(a, c); break; }
+    if (cg && info.z < 0) ++ph;
+    tc::tc_fence_after();
+    RowSystem<KA, REG> sys;
+    float bm;
+    {
+      float b16[16];
+      tc::tmem_ld16(tA + bcol, b16);  // b_u sits in column c_r = ld of D
+      bm = 0.f;
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q == bq) bm = b16[q];
+    }
+    sys.load(tA);
+    if constexpr (REG) {
+      // the accumulator may be overwritten now
+      tc::tc_fence_before();
+      tc::mbar_arrive(&c.acc_empty[ab]);
+    }
+    if (info.z >= 0) {
+      // A chunk of a split row: store the partial sums; the chunk that
+      // finishes last adds all of them, in chunk order, and solves the row.
+      float *P = plan.partial + ((size_t)info.z * 128 + m) * plan.part_ld;
+      sys.save_partial(P, live, 0);
+      __stcg(P + NP, live ? bm : 0.f);
+      __threadfence();
+      B.sync();
+      if (lt == 0) {
+        const unsigned done = atomicAdd(&plan.heavy_count[info.w], 1u) + 1;
+        bad[1] = done == (unsigned)plan.heavy_nchunks[info.w] ? 1 : 0;
+      }
+      B.sync();
+      const bool last = bad[1] != 0;
+      B.sync();
+      if (!last) {
+        if constexpr (!REG) {
+          tc::tc_fence_before();
+          tc::mbar_arrive(&c.acc_empty[ab]);
+        }
+        continue;
+      }
+      __threadfence();
+      const int base = plan.heavy_base[info.w], nch = plan.heavy_nchunks[info.w];
+      if constexpr (REG) {
+        sys.clear();
+        for (int ch = 0; ch < nch; ++ch)
+          sys.add(plan.partial + ((size_t)(base + ch) * 128 + m) * plan.part_ld);
+      } else {
+        sys.sum_partials(plan.partial, base, nch, m, plan.part_ld);
+      }
+      bm = 0.f;
+      for (int ch = 0; ch < nch; ++ch)
+        bm += __ldcg(plan.partial + ((size_t)(base + ch) * 128 + m) * plan.part_ld + NP);
+      if (lt == 0) plan.heavy_count[info.w] = 0;  // ready for the next half-step
+      x = (live && sv.x0) ? sv.x0[u * sv.ld_x0 + m] : 0.f;
+      if (!isfinite(x)) x = 0.f;
+      if (cg) {
+        vbuf(0)[m] = x;
+        B.sync();
+        ++ph;
+      }
+    }
+    // Rows past f carry no unknowns (row c_r of D holds b_u^T): a padding
+    // thread's values are cleared, with one predicate per thread. Columns past
+    // f need no clearing: they meet broadcast entries that are zero (every
+    // published vector is zero past f), and the Cholesky tile is patched below.
+    if constexpr (REG) {
+      if (!live) sys.clear();
+    }
+    if (!live) bm = 0.f;
+    uint32_t flags = 0;
+    bool solved = false;
+    float xm = 0.f;
+    if (cg) {
+      float dinv = live ? 1.f : 0.f;
+      if (L::kChol && sv.jacobi) {  // (wide instances are not launched with Jacobi)
+        // the diagonal entry A[m][m] sits at a thread-dependent column: go
+        // through the (still unused) Cholesky tile for it (every thread calls
+        // store: its TMEM loads are warp-collective)
+        sys.store(S + (m < FP ? m : 0) * LDS, m < FP);
+        __syncwarp();
+        if (live) dinv = 1.f / (S[m * LDS + m] + reg);
+      }
+      float r = bm;
+      if (sv.x0) {
+        // Scale the warm start optimally along its own direction:
+        // alpha = x0.b / x0.A x0 minimises the A-norm error of alpha * x0, so
+        // the start is never worse than zero in that norm. x0 was published
+        // with the accumulator vote (or after the split row's sums).
+        float q0 = sys.mv(pv + ((ph - 1) & 1) * 256, reg, x);
+        if (!live) q0 = 0.f;
+        group_partial2(x * bm, x * q0, rbuf(), lt);
+        B.sync();
+        const float2 xs = group_read2(rbuf());
+        ++ph;
+        float sc = xs.x / xs.y;
+        if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
+        x *= sc;
+        r = bm - sc * q0;
+      }
+      if (!live) r = 0.f;
+      float z = dinv * r;
+      // z is broadcast through the barrier that sums r.z, r.r and b.b
+      vbuf(0)[m] = z;
+      group_partial4(make_float4(r * z, r * r, bm * bm, 0.f), rbuf(), lt);
+      B.sync();
+      const float4 t0 = group_read4(rbuf());
+      const float *vz = vbuf(0);
+      ++ph;
+      float gamma = t0.x;
+      const float bb = t0.z, target = sv.cg_tol2 * bb;
+      if (lt == 0 && bb > 0.f) cnt[5] += (unsigned long long)(1e6f * sqrtf(t0.y / bb));
+      bool conv = t0.y <= target;
+      int it = 0;
+      float p = 0.f, w = 0.f, beta = 0.f;
+      // Conjugate gradients, two barriers a step: A p is carried by the
+      // recurrence A p_k = A z_k + beta_k A p_{k-1} (p_k = z_k + beta_k p_{k-1}),
+      // so the product is taken of z, which is broadcast through the same
+      // barrier that sums r.z and r.r.
+      while (!conv && it < sv.cg_max_steps) {
+        float az = sys.mv(vz, reg, z);
+        if (!live) az = 0.f;
+        p = fmaf(beta, p, z);
+        w = fmaf(beta, w, az);
+        group_partial1(p * w, rbuf(), lt);
+        B.sync();
+        const float pq = group_read1(rbuf());
+        ++ph;
+        if (!(pq > 0.f)) break;  // not positive definite along p: fall back
+        const float alpha = __fdividef(gamma, pq);
+        x = fmaf(alpha, p, x);
+        r = fmaf(-alpha, w, r);
+        z = dinv * r;
+        vbuf(0)[m] = z;
+        group_partial2(r * z, r * r, rbuf(), lt);
+        B.sync();
+        const float2 t = group_read2(rbuf());
+        vz = vbuf(0);
+        ++ph;
+        ++it;
+        conv = t.y <= target;
+        beta = __fdividef(t.x, gamma);
+        gamma = t.x;
+      }
+      if (lt == 0) cnt[3] += it;
+      if (conv) {
+        solved = true;
+        xm = x;
+      } else {
+        flags |= kRowCgFallback;
+        if (lt == 0) ++cnt[4];
+      }
+    }
+    if constexpr (!L::kChol) {
+      if (!solved) {
+        // no tile for this rank: the row goes to the post-pass of the
+        // one-CTA-per-row kernel, which writes its result and status
+        if (lt == 0) plan.fb_rows[atomicAdd(plan.fb_count, 1)] = (int)u;
+        if constexpr (!REG) {
+          tc::tc_fence_before();
+          tc::mbar_arrive(&c.acc_empty[ab]);
+        }
+        continue;
+      }
+    }
+    if (lt == 0) ++cnt[0];
+    if constexpr (L::kChol) {
+      if (!solved) {
+        // the system into the tile for the register-tile Cholesky
+        B.sync();  // the tile, dg, bv and xv are free; the last reduction has been read
+        float *Sr = S + (m < FP ? m : 0) * LDS;
+        sys.store(Sr, live);  // every thread (warp-collective TMEM loads); live rows store
+        if (m < FP) {
+          if (live)
+            for (int cc = f; cc < FP; ++cc) Sr[cc] = 0.f;  // padding (and the b_u column)
+          bv[m] = bm;
+        }
+        __syncwarp();
+        if (m < FP && !live)
+          for (int cc = 0; cc < FP; ++cc) S[m * LDS + cc] = cc == m ? 1.f : 0.f;  // identity block
+        B.sync();
+        const int res = ws_cholesky<FP>(S, dg, bv, xv, tmp, rd, red + 32, bad, f, reg, a.refine_tol, B);
+        if (res == 1) {
+          flags |= kRowNotSPD;
+          if (lt == 0) ++cnt[2];
+        } else if (res == 2) {
+          flags |= kRowRefinedF64;
+          if (lt == 0) ++cnt[1];
+        }
+        if (live) xm = xv[m];
+        B.sync();
+      }
+    }
+    if constexpr (!REG) {
+      // the accumulator may be overwritten now
+      tc::tc_fence_before();
+      tc::mbar_arrive(&c.acc_empty[ab]);
+    }
+    if (live) {
+      a.dst[u * a.ld_dst + m] = xm;
+      if (a.dst_lp) reinterpret_cast<LP *>(a.dst_lp)[u * a.ld_dst_lp + m] = LP(xm);
+    }
+    if (a.row_flags && lt == 0) a.row_flags[u] = flags;
+  }
+  if (a.counters && lt == 0) {
+    atomicAdd(&a.counters->rows, cnt[0]);
+    if (cnt[1]) atomicAdd(&a.counters->refined, cnt[1]);
+    if (cnt[2]) atomicAdd(&a.counters->not_spd, cnt[2]);
+    if (cnt[3]) atomicAdd(&a.counters->cg_steps, cnt[3]);
+    if (cnt[4]) atomicAdd(&a.counters->cg_fallback, cnt[4]);
+    if (cnt[5]) atomicAdd(&a.counters->r0_micro, cnt[5]);
+  }
+}
+
 template <int FP, int NP, typename LP, int NG>
 __global__ void __launch_bounds__(ws::threads<NG>(), 1)
 rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_arg) {
@@ -870,23 +1434,22 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
   c.full = reinterpret_cast<uint64_t *>(ctrl);
   c.empty = c.full + ws::NS;
   c.acc_full = c.empty + ws::NS;
-  c.acc_empty = c.acc_full + ws::kAcc;
-  c.row_full = c.acc_empty + ws::kAcc;
+  c.acc_empty = c.acc_full + ws::kMaxAcc;
+  c.row_full = c.acc_empty + ws::kMaxAcc;
   c.row_empty = c.row_full + ws::kRowSlots;
   c.drain = c.row_empty + ws::kRowSlots;
   c.stage_info = reinterpret_cast<int4 *>(ctrl + L::kBars);
   c.row_info = c.stage_info + ws::NS;
   c.misc = reinterpret_cast<volatile int *>(c.row_info + ws::kRowSlots);
   const int tid = threadIdx.x, warp = tid >> 5;
-  WsPlan plan = plan_arg;
-  if (plan.nitems_dev) plan.nitems = *plan.nitems_dev;  // built on the device
+  const WsPlan &plan = plan_arg;  // stays in the parameter space
 
   if (tid == 0) {
     for (int i = 0; i < ws::NS; ++i) {
       tc::mbar_init(&c.full[i], ws::kFullCount);
       tc::mbar_init(&c.empty[i], 1);
     }
-    for (int b = 0; b < ws::kAcc; ++b) {
+    for (int b = 0; b < ws::kMaxAcc; ++b) {
       tc::mbar_init(&c.acc_full[b], 1);
       tc::mbar_init(&c.acc_empty[b], 128);
     }
@@ -904,7 +1467,7 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
                  "r"(ws::kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  for (int q = tid; q < ws::NS * ws::kStageBytes / 16; q += ws::threads<NG>())
+  for (int q = tid; q < ws::NS * ws::Dims<FP>::kStageBytes / 16; q += ws::threads<NG>())
     reinterpret_cast<uint4 *>(base)[q] = make_uint4(0, 0, 0, 0);
   tc::fence_proxy_async();
   tc::tc_fence_before();
@@ -914,16 +1477,20 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
   unsigned long long n_empty = 0;
 
   if (warp == ws::mma_warp<NG>()) {
-    if ((tid & 31) == 0) ws_mma(a, c, base, tmem, idesc);
+    if ((tid & 31) == 0) ws_mma<FP>(a, c, base, tmem, idesc);
     __syncwarp();
   } else if (warp == ws::prod_warp<NG>() || warp >= ws::prod_warp<NG>() + 2) {
     const int k = warp == ws::prod_warp<NG>() ? 0 : warp - ws::prod_warp<NG>() - 1;
-    ws_produce<LP, NG>(a, plan, g, c, base, base + L::oRing + (size_t)k * ws::DI * ws::kRingSlot, k,
+    ws_produce<FP, LP, NG>(a, plan, g, c, base, base + L::oRing + (size_t)k * ws::DI * ws::kRingSlot, k,
                        n_empty);
     if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
   } else if (warp < 4 * NG) {
-    ws_solve<FP, NP, LP, NG>(a, plan, sv, c, base + L::oSolver + (size_t)(warp >> 2) * L::kSolver,
-                             tmem, warp >> 2);
+    unsigned char *mem = base + L::oSolver + (size_t)(warp >> 2) * L::kSolver;
+    // Ranks up to 112: the system stays in its TMEM accumulator. Above: the
+    // wide solver, rows in registers with one solver warpgroup (255 registers
+    // a thread hold a row without spilling), in TMEM otherwise.
+    if constexpr (!ws::Dims<FP>::kWide) ws_solve<FP, NP, LP, NG>(a, plan, sv, c, mem, tmem, warp >> 2);
+    else ws_solve_wide<FP, NP, LP, NG, NG == 1>(a, plan, sv, c, mem, tmem, warp >> 2);
   }
   tc::tc_fence_before();
   __syncthreads();
@@ -934,7 +1501,10 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
   }
 }
 
-bool tc_ws_supported(int f) { return f >= 16 && f <= 112; }
+bool tc_ws_supported(int f) { return f >= 16 && f <= 128; }
+bool tc_ws_takes(int f, int solver, int jacobi) {
+  return tc_ws_supported(f) && (f <= 112 || (solver == 1 && !jacobi));
+}
 
 // Load the kernel instance for (f, lp_kind, groups) and set its shared-memory
 // attribute without launching it, so that its first real launch (for example
@@ -945,6 +1515,7 @@ cudaError_t prepare_rows_tc_ws(int f, int lp_kind, int groups) {
   a.ld_src = tc_padded_ld(f);
   a.src = reinterpret_cast<const void *>(uintptr_t(256));  // never dereferenced
   TcSolve sv{};
+  sv.solver = 1;  // every instance takes CG (wide ones only CG)
   sv.groups = groups;
   sv.prepare = 1;
   WsPlan plan;
@@ -961,8 +1532,10 @@ static cudaError_t launch_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
   static_assert(L::kTotal <= 232448, "227 KB of shared memory per CTA");
   WsGeom g;
   g.nj = a.ld_src / 8;
-  if (a.ld_src % 8 != 0 || a.ld_src > 120 || NP < a.f || FP < a.f || plan.part_ld < NP + 1)
+  constexpr int kMaxLd = ws::Dims<FP>::kWide ? 136 : 120;  // c_r = ld within the stage's atoms
+  if (a.ld_src % 8 != 0 || a.ld_src > kMaxLd || NP < a.f || FP < a.f || plan.part_ld < NP + 1)
     return cudaErrorInvalidValue;
+  if (ws::Dims<FP>::kWide && (sv.solver != 1 || sv.jacobi)) return cudaErrorNotSupported;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
   auto kern = rows_tc_ws_kernel<FP, NP, LP, NG>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kTotal);
@@ -1005,6 +1578,7 @@ cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
     case 96: return launch_ws_np<104, 96>(a, lp_kind, sv, plan, num_sms, st);
     case 112: return f <= 104 ? launch_ws_np<104, 112>(a, lp_kind, sv, plan, num_sms, st)
                               : launch_ws_np<112, 112>(a, lp_kind, sv, plan, num_sms, st);
+    case 128: return launch_ws_np<128, 128>(a, lp_kind, sv, plan, num_sms, st);
     default: return cudaErrorNotSupported;
   }
 }
@@ -1066,8 +1640,16 @@ __device__ __forceinline__ int64_t plan_deg(const PlanDev &p, int64_t r) {
   const int64_t d = p.ptr[p.begin + r + 1] - p.ptr[p.begin + r];
   return d > 0 ? d : 0;
 }
+// Size bins, largest first: items shorter than kPlanExact ratings (most rows
+// of power-law matrices) get a bin of their own size, so they are ordered
+// exactly; longer ones share kPlanBins - kPlanExact bins spread linearly up to
+// `split`.
+constexpr int kPlanExact = 3072;
 __device__ __forceinline__ int plan_bin(int64_t size, int64_t split) {
-  return (int)((split - size) * kPlanBins / (split + 1));
+  if (size < kPlanExact) return kPlanBins - 1 - (int)size;
+  constexpr int kCoarse = kPlanBins - kPlanExact;
+  const int64_t span = split - kPlanExact + 1;  // split >= 8192 > kPlanExact
+  return (int)((split - size) * kCoarse / span);
 }
 __device__ __forceinline__ void plan_rows_of_block(const PlanDev &p, int64_t &r0, int64_t &r1) {
   const int64_t per = (p.count + gridDim.x - 1) / gridDim.x;
@@ -1142,6 +1724,10 @@ __global__ void __launch_bounds__(1024) plan_scan_kernel(PlanDev p) {
   }
 }
 
+// Rank k (largest first) goes to CTA c = k mod G as that CTA's q-th largest
+// of its nc items; within the CTA the order zigzags between its largest and
+// smallest items (slots 0, 2, 4, ... take the largest, 1, 3, 5, ... the
+// smallest).
 __device__ __forceinline__ void plan_put(const PlanDev &p, int64_t k, int64_t N, const WorkItem &w) {
   const int64_t G = p.grid, c = k % G, q = k / G, nc = (N - c + G - 1) / G;
   const int64_t j = q < (nc + 1) / 2 ? 2 * q : 2 * (nc - 1 - q) + 1;  // zigzag slot
@@ -1199,7 +1785,7 @@ __global__ void __launch_bounds__(kPlanThreads) plan_place_kernel(PlanDev p) {
 }
 
 struct PlanLayout {
-  size_t oHdr, oHist, oCur, oHr, oHn, oHb, oHc, oItems, oPart, oChol, total;
+  size_t oHdr, oHist, oCur, oHr, oHn, oHb, oHc, oItems, oPart, oChol, oFb, oFbc, total;
   PlanLayout(int64_t count, int grid, int np) {
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     // A row of d > split ratings becomes ceil(d / split) < d / split + 1
@@ -1218,6 +1804,8 @@ struct PlanLayout {
     oItems = o; o += al(sizeof(WorkItem) * imax);
     oPart = o; o += al(sizeof(float) * smax * 128 * (size_t)(np + 4) + 16);
     oChol = o; o += al(sizeof(float) * (size_t)grid * ws::kMaxGroups * kCholFloats);
+    oFb = o; o += al(4 * (size_t)count);  // rows deferred to the post-pass (ranks above 112)
+    oFbc = o; o += al(8);
     total = o;
   }
 };
@@ -1281,6 +1869,9 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
   plan->partial = reinterpret_cast<float *>(d + L.oPart);
   plan->chol = reinterpret_cast<float *>(d + L.oChol);
   plan->ctas = grid;
+  plan->fb_rows = reinterpret_cast<int *>(d + L.oFb);
+  plan->fb_count = reinterpret_cast<int *>(d + L.oFbc);
+  plan->rows = count;
   return cudaSuccess;
 }
 

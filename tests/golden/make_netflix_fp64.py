@@ -35,15 +35,18 @@ N_SAMPLE = 256
 
 
 def checksums(r, th0):
-    """Order-sensitive checksums of the generated inputs (float64 / int64 sums
-    weighted by position, so a permuted or shifted array changes them)."""
+    """Order-sensitive checksums of the generated inputs: the sum, modulo 2^64,
+    of each array's bit patterns weighted by position. Integer arithmetic, so
+    every machine gets the same value for the same bytes."""
     def wsum(a):
-        a = np.asarray(a, np.float64).ravel()
-        w = (np.arange(a.size, dtype=np.float64) % 1009.0) + 1.0
-        return float(np.dot(a, w))
+        a = np.ascontiguousarray(a)
+        bits = a.view(np.uint64 if a.itemsize == 8 else np.uint32).ravel().astype(np.uint64)
+        w = (np.arange(bits.size, dtype=np.uint64) % np.uint64(1009)) + np.uint64(1)
+        with np.errstate(over="ignore"):
+            return int(np.sum(bits * w, dtype=np.uint64))
     return np.array([r.m, r.n, r.nnz, len(r.test_r), wsum(r.csr_ptr), wsum(r.csr_col),
                      wsum(r.csr_val), wsum(r.test_u), wsum(r.test_i), wsum(r.test_r),
-                     wsum(th0)], np.float64)
+                     wsum(th0)], np.uint64)
 
 
 def main(outdir):

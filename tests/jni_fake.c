@@ -13,6 +13,11 @@ static int live_critical = 0;
 
 static void *FindClass(void *env, const char *name) { (void)env; (void)name; return (void *)0x1; }
 static void DeleteLocalRef(void *env, void *o) { (void)env; (void)o; }
+static int frames = 0, max_frames = 0;
+static int PushLocalFrame(void *env, int capacity) {
+  (void)env; (void)capacity; if (++frames > max_frames) max_frames = frames; return 0;
+}
+static void *PopLocalFrame(void *env, void *result) { (void)env; --frames; return result; }
 static int GetArrayLength(void *env, jarr *a) { (void)env; return a->len; }
 static jarr *new_arr(int kind, int len, size_t elem) {
   jarr *a = (jarr *)calloc(1, sizeof(jarr));
@@ -25,6 +30,9 @@ static jarr *NewObjectArray(void *env, int len, void *cls, void *init) {
 static void *GetObjectArrayElement(void *env, jarr *a, int i) { (void)env; return ((void **)a->data)[i]; }
 static void SetObjectArrayElement(void *env, jarr *a, int i, void *v) { (void)env; ((void **)a->data)[i] = v; }
 static jarr *NewFloatArray(void *env, int len) { (void)env; return new_arr(2, len, sizeof(float)); }
+static void GetFloatArrayRegion(void *env, jarr *a, int start, int len, float *buf) {
+  (void)env; memcpy(buf, (float *)a->data + start, sizeof(float) * (size_t)len);
+}
 static void SetFloatArrayRegion(void *env, jarr *a, int start, int len, const float *buf) {
   (void)env; memcpy((float *)a->data + start, buf, sizeof(float) * (size_t)len);
 }
@@ -37,12 +45,15 @@ static void ReleasePrimitiveArrayCritical(void *env, jarr *a, void *p, int mode)
 
 void *fake_env(void) {
   table[6] = (void *)FindClass;
+  table[19] = (void *)PushLocalFrame;
+  table[20] = (void *)PopLocalFrame;
   table[23] = (void *)DeleteLocalRef;
   table[171] = (void *)GetArrayLength;
   table[172] = (void *)NewObjectArray;
   table[173] = (void *)GetObjectArrayElement;
   table[174] = (void *)SetObjectArrayElement;
   table[181] = (void *)NewFloatArray;
+  table[205] = (void *)GetFloatArrayRegion;
   table[213] = (void *)SetFloatArrayRegion;
   table[222] = (void *)GetPrimitiveArrayCritical;
   table[223] = (void *)ReleasePrimitiveArrayCritical;
@@ -64,3 +75,5 @@ int fake_length(jarr *a) { return a->len; }
 void *fake_get(jarr *a, int i) { return ((void **)a->data)[i]; }
 float *fake_float_data(jarr *a) { return (float *)a->data; }
 int fake_live_critical(void) { return live_critical; }
+int fake_open_frames(void) { return frames; }
+int fake_max_frames(void) { return max_frames; }

@@ -39,6 +39,8 @@ def _fake():
     lib.fake_float_data.restype = ctypes.POINTER(ctypes.c_float)
     lib.fake_float_data.argtypes = [vp]
     lib.fake_live_critical.restype = ctypes.c_int
+    lib.fake_open_frames.restype = ctypes.c_int
+    lib.fake_max_frames.restype = ctypes.c_int
     return lib
 
 
@@ -78,11 +80,21 @@ def test_jni_doALSWithCSR_through_fake_env():
     X = np.array([np.ctypeslib.as_array(fk.fake_float_data(fk.fake_get(out, i)), (f,))
                   for i in range(r.m)])
     assert fk.fake_live_critical() == 0  # every critical section was released
+    assert fk.fake_open_frames() == 0 and fk.fake_max_frames() >= 1  # local frames balanced
     X_ref, _ = O.half_step(r.csr_ptr, r.csr_col, r.csr_val, th, 0.05)
     err = np.linalg.norm(X - X_ref, axis=1) / np.maximum(np.linalg.norm(X_ref, axis=1), 1e-30)
     assert err.max() < 1e-3
     X2 = A.do_als_with_csr(ptr32, r.csr_col, r.csr_val, th, r.m, r.n, f, 0.05)
     assert np.array_equal(X, X2)
+    # a second call reuses the shim's pooled pinned buffers and stream
+    jrow = fk.fake_int_array(len(ptr32), ptr32.ctypes.data)
+    jcol = fk.fake_int_array(len(r.csr_col), r.csr_col.ctypes.data)
+    jval = fk.fake_float_array(len(r.csr_val), r.csr_val.ctypes.data)
+    out2 = fn(fk.fake_env(), None, r.m, r.n, f, r.nnz, 0.05, outer, jrow, jcol, jval)
+    assert out2 and fk.fake_open_frames() == 0
+    X3 = np.array([np.ctypeslib.as_array(fk.fake_float_data(fk.fake_get(out2, i)), (f,))
+                   for i in range(r.m)])
+    assert np.array_equal(X, X3)
 
 
 def _no_gpu():

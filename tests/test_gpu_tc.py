@@ -112,13 +112,16 @@ def test_tc_training_rmse_close_to_fp64():
         M.close()
 
 
-@pytest.mark.parametrize("f", [100, 48])
+@pytest.mark.parametrize("f", [100, 48, 120, 128])
 def test_solver_groups_agree_with_oracle(f):
     """The hot kernel with 1, 2 and 3 solver warpgroups (and the autotuner) on
     a matrix with multi-stage rows and item rows long enough to be split
     across CTAs: every configuration gives the same bits, and both sides match
     the FP64 oracle on the BF16-rounded factors (tolerance 1e-3). This covers
-    the two producers' alternate stages and the per-group row hand-over."""
+    the producers' alternate stages and the per-group row hand-over, and both
+    placements of a row's system (registers with one or two warpgroups up to
+    f = 112 and with one above it, TMEM otherwise), which must agree bit for
+    bit. f = 120 and 128 use the three-atom stages and three accumulators."""
     r = A.synth(A.scaled_config("netflix", 0.1), seed=7)
     assert np.diff(r.csc_ptr).max() > 8192  # some item rows are split
     th = A.init_factors(r.n, f, 11)
@@ -141,3 +144,51 @@ def test_solver_groups_agree_with_oracle(f):
     assert rel_rows(X, Xr).max() < TOL
     Tr, _ = O.half_step(r.csc_ptr, r.csc_row, r.csc_val, rnd(X, A.PREC_BF16), 0.05)
     assert rel_rows(T, Tr).max() < TOL
+
+
+@pytest.mark.parametrize("f", [100, 128])
+@pytest.mark.parametrize("ng", [1, 2, 3])
+def test_cg_fallback_rows_match_oracle(f, ng):
+    """CG limited to two steps, so most rows cannot finish: up to f = 112 they
+    are solved by the kernel's own register-tile Cholesky (the system copied
+    from registers or from TMEM into the tile), above it by the post-pass of
+    the one-CTA-per-row kernel. Every row still matches the FP64 oracle on
+    the BF16-rounded factors (1e-3) and carries the CG-fallback status bit;
+    Jacobi-preconditioned CG (f = 100) takes the same fallback."""
+    r = A.synth(A.scaled_config("netflix", 0.03), seed=17)
+    th = A.init_factors(r.n, f, 19)
+    Xr, _ = O.half_step(r.csr_ptr, r.csr_col, r.csr_val, rnd(th, A.PREC_BF16), 0.05)
+    keep = np.diff(r.csr_ptr) > 0
+    for jac in ((0, 1) if f <= 112 else (0,)):
+        M = A.Model(r, f, A.options(precision=A.PREC_BF16, solver=A.SOLVER_CG, warm_start=A.WARM_ZERO,
+                                    cg_max_steps=2, cg_jacobi=jac, solver_groups=ng), theta0=th)
+        M.half_step(A.SIDE_USERS, 0.05)
+        X = M.factors()[0].cpu().numpy()
+        flags = M.row_flags(A.SIDE_USERS).cpu().numpy()
+        st = M.stats()
+        M.close()
+        assert st["kernel_errors"] == 0 and st["rows_solved"] == r.m, st
+        assert st["cg_fallbacks"] > r.m // 2, st
+        fb = (flags & A.ROW_CG_FALLBACK) != 0
+        assert fb.sum() == st["cg_fallbacks"]
+        assert rel_rows(X, Xr)[keep].max() < TOL, (jac, rel_rows(X, Xr)[keep].max())
+
+
+def test_wide_rank_runs_on_the_warp_specialised_kernel():
+    """At f = 128 the CG form runs on the warp-specialised kernel: its
+    autotuner (which only that kernel has) settles on a warpgroup count for
+    each side after three half-steps, and the result matches the oracle."""
+    r = A.synth(A.scaled_config("netflix", 0.05), seed=23)
+    f = 128
+    th = A.init_factors(r.n, f, 29)
+    M = A.Model(r, f, A.options(precision=A.PREC_BF16, solver=A.SOLVER_CG, warm_start=A.WARM_ZERO),
+                theta0=th)
+    for _ in range(3):
+        M.half_step(A.SIDE_USERS, 0.05)
+    X = M.factors()[0].cpu().numpy()
+    st = M.stats()
+    M.close()
+    assert st["solver_groups"][0] in (1, 2), st
+    Xr, _ = O.half_step(r.csr_ptr, r.csr_col, r.csr_val, rnd(th, A.PREC_BF16), 0.05)
+    keep = np.diff(r.csr_ptr) > 0
+    assert rel_rows(X, Xr)[keep].max() < TOL
