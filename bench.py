@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip timing the FP32 Cholesky and learned-start forms beside the default")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample time")
     return p.parse_args()
 
@@ -251,9 +253,11 @@ def run_reference(args):
 # Per-launch DRAM traffic of the rows kernel at the default workload (the
 # Netflix shape, BF16 CG, previous iterate), from one ncu capture of the same
 # command at full size (dram__bytes_read.sum + dram__bytes_write.sum, one pass;
-# profiles/rows_tc_ws_netflix_dram.txt). None for other workloads.
-DRAM_PER_LAUNCH = None
-DRAM_SOURCE = None
+# profiles/rows_tc_ws_netflix_dram.txt): the mean of the users launch (1.468 GB)
+# and the items launch (3.371 GB). None for other workloads.
+DRAM_PER_LAUNCH = 2.420e9
+DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, full-size workload, 4th iteration: "
+               "users 1.468e9, items 3.371e9 bytes")
 
 FIXTURE = os.path.join(ROOT, "tests", "golden", "netflix_f100_fp64.npz")
 RESTART = 10  # iterations of one training run (the workload's iteration count)
@@ -465,7 +469,7 @@ def run_engine(args):
     # The other forms of the north-star comparison on the same GPU and matrix:
     # the plain FP32 Cholesky form and the learned warm start (its net trains
     # during iterations 1-3, which are its warm-up here).
-    if rank == 0 and world == 1 and args.precision != "fp32" and not args.graph:
+    if rank == 0 and world == 1 and args.precision != "fp32" and not args.graph and not args.no_forms:
         forms = {}
         for name, o2, warmup_it, timed_it in (
                 ("fp32_cholesky", A.options(precision=A.PREC_FP32, solver=A.SOLVER_CHOLESKY), 1, 3),

@@ -361,7 +361,9 @@ __global__ void __launch_bounds__(256) features_plan_kernel(WsPlan plan, int f, 
   __shared__ float tot[256];
   __shared__ int last;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, h = lane >> 4, j = lane & 15;
-  const int nj = ld_src / 8;
+  // 16-byte pieces that hold columns below f (at most 16 for f <= 128; the
+  // stride may have one more piece of padding, which the features never read)
+  const int nj = min(ld_src / 8, (f + 7) / 8);
   const int64_t nitems = plan.nitems_dev ? *plan.nitems_dev : plan.nitems;
   for (int64_t idx = blockIdx.x; idx < nitems; idx += gridDim.x) {
     const WorkItem it = plan.items[idx];
@@ -775,7 +777,7 @@ cudaError_t mlp_features_plan(const WsPlan &plan, int f, const int32_t *col, con
                               const void *src, int ld_src, int lp_kind, void *F, int ldf,
                               cudaStream_t st) {
   if (plan.nitems <= 0) return cudaSuccess;
-  if (f > 128 || ld_src % 8 != 0 || ld_src > 128 || (reinterpret_cast<uintptr_t>(src) & 15) != 0 ||
+  if (f > 128 || ld_src % 8 != 0 || ld_src < f || (reinterpret_cast<uintptr_t>(src) & 15) != 0 ||
       plan.part_ld * 128 < 256 || (lp_kind != kLpBf16 && lp_kind != kLpFp16))
     return cudaErrorNotSupported;
   const unsigned grid = (unsigned)std::min<int64_t>(plan.nitems, (int64_t)device_sm_count() * 8);

@@ -109,7 +109,7 @@ def test_learned_warm_start_gain_in_als(f):
 
 
 @pytest.mark.parametrize("f,prec", [(100, A.PREC_BF16), (16, A.PREC_FP16), (33, A.PREC_BF16),
-                                    (20, A.PREC_FP32)])
+                                    (20, A.PREC_FP32), (128, A.PREC_BF16), (120, A.PREC_FP16)])
 def test_features_match_numpy(f, prec):
     """Row features [b_u / n_u, diag(A_u) / n_u, log1p(n_u) / 8] against numpy
     on the same 16-bit (or FP32) factors: empty rows, short rows, rows long
