@@ -115,6 +115,7 @@ _sig(lib.als_train, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i
 _sig(lib.doALSWithCSR, None, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int,
      ctypes.c_int, ctypes.c_long, c_f32, ctypes.c_int)
 _sig(lib.als_set_dropin_options, c_i32, c_vp)
+_sig(lib.als_debug_withhold_first_row, c_i32, c_i32)
 _sig(lib.als_get_dropin_options, c_i32, c_vp)
 # mallocBest / freeBest keep the reference's C++ linkage; these are their C names
 _sig(lib.als_malloc_best, ctypes.c_int, c_vp, c_sz)

@@ -25,6 +25,11 @@ using namespace als;
 namespace {
 
 thread_local std::string g_last_error;
+
+std::atomic<bool> &debug_withhold() {
+  static std::atomic<bool> flag{false};
+  return flag;
+}
 std::mutex g_dropin_mu;
 als_options g_dropin;       // set on first use from als_default_options
 bool g_dropin_set = false;
@@ -208,6 +213,11 @@ int als_set_dropin_options(const als_options *o) {
   return ALS_OK;
 }
 const char *als_version(void) { return "als_b200 1.0 (sm_100a)"; }
+
+int als_debug_withhold_first_row(int32_t enable) {
+  debug_withhold().store(enable != 0);
+  return ALS_OK;
+}
 
 int als_model_create(als_model **out, int64_t m, int64_t n, int32_t f, int64_t nnz,
                      const int64_t *csr_ptr, const int32_t *csr_col, const float *csr_val,
@@ -896,6 +906,8 @@ static void throw_cuda(cudaError_t e, const char *where) {
 }
 
 namespace als {
+bool debug_take_withhold() { return debug_withhold().exchange(false); }
+
 // The drop-in call's check of the kernels' error word after a half-step:
 // results of a half-step whose kernel gave up a bounded wait (bit 1), or whose
 // work plan was rejected for malformed row pointers (bit 2), are incomplete,

@@ -35,7 +35,12 @@ struct TcSolve {
   int groups;          // solver warpgroups per CTA of the warp-specialised kernel (1, 2 or 3)
   int prepare;         // 1: only load the kernel instance and set its attributes
   uint32_t flags_or;   // status bits added to every row's word (one-CTA-per-row kernel)
+  int withhold_first;  // test support: CTA 0 withholds its first item's accumulator completion
 };
+
+// Test support (als_debug_withhold_first_row): one-shot; the next launch of
+// the warp-specialised kernel takes it.
+bool debug_take_withhold();
 
 // Work list of the warp-specialised kernel, planned on the host per side:
 // one item per row, or one per chunk of a row split across CTAs.

@@ -461,6 +461,14 @@ cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_ma
       cudaError_t e = cudaMemsetAsync(plan->fb_count, 0, 2 * sizeof(int), st);
       if (e != cudaSuccess) return e;
     }
+    // The split rows' chunk counters start at zero: the kernel's last chunk
+    // resets its row's counter, but a launch that gave up a bounded wait may
+    // have left some part-way.
+    if (plan->heavy_count && plan->ctas > 0) {
+      cudaError_t e = cudaMemsetAsync(plan->heavy_count, 0, sizeof(unsigned) * (4 * (size_t)plan->ctas + 1), st);
+      if (e != cudaSuccess) return e;
+    }
+    sv.withhold_first = debug_take_withhold() ? 1 : 0;
     cudaError_t e = launch_rows_tc_ws(a, lp_kind, sv, *plan, num_sms, st);
     if (e != cudaSuccess || !post || sv.prepare) return e;
     // The post-pass: the rows CG did not finish (listed by the warp-specialised

@@ -485,7 +485,10 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
 // ---------------------------------------------------------------------------
 template <int FP>
 __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages, uint32_t tmem,
-                       uint32_t idesc) {
+                       uint32_t idesc, bool withhold_first) {
+  // (test support: with withhold_first, the first item's accumulator is never
+  // marked full, so its solver's bounded wait runs out)
+  long long items_done = 0;
   const uint32_t lbo = (ws::KS / 8) * 1024, sbo = 1024;
   const uint32_t st0 = tc::smem_u32(stages);
   unsigned full_par = 0, acc_used = 0, acc_par = 0;
@@ -519,7 +522,10 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
                   (first && kk == 0) ? 0u : 1u);
     }
     tc::mma_commit(&c.empty[slot]);
-    if (last) tc::mma_commit(&c.acc_full[b]);
+    if (last) {
+      if (!(withhold_first && items_done == 0)) tc::mma_commit(&c.acc_full[b]);
+      ++items_done;
+    }
     slot = slot + 1 == ws::NS ? 0 : slot + 1;
   }
   if (!ok) ws_abort(a, c);
@@ -1477,7 +1483,7 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
   unsigned long long n_empty = 0;
 
   if (warp == ws::mma_warp<NG>()) {
-    if ((tid & 31) == 0) ws_mma<FP>(a, c, base, tmem, idesc);
+    if ((tid & 31) == 0) ws_mma<FP>(a, c, base, tmem, idesc, sv.withhold_first && blockIdx.x == 0);
     __syncwarp();
   } else if (warp == ws::prod_warp<NG>() || warp >= ws::prod_warp<NG>() + 2) {
     const int k = warp == ws::prod_warp<NG>() ? 0 : warp - ws::prod_warp<NG>() - 1;

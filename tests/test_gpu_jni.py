@@ -167,3 +167,42 @@ def test_jni_error_inside_dropin_returns_null():
     # a valid call afterwards still works
     X = A.do_als_with_csr(ptr, col, val, th[:, :16].copy(), m, n, 16, 0.05)
     assert np.isfinite(X).all()
+
+
+@pytest.mark.gpu
+def test_jni_kernel_timeout_returns_null():
+    """A half-step whose kernel gives up a bounded wait (forced by the test
+    switch) makes doALSWithCSR throw instead of returning incomplete rows; the
+    Spark shim reports it and returns null, and the next call is correct."""
+    fk = _fake()
+    r = A.synth(A.scaled_config("ml1m", 0.1), seed=8)
+    f = 32
+    th = A.init_factors(r.n, f, 1)
+    outer = fk.fake_object_array(1)
+    blk = fk.fake_object_array(r.n)
+    keep = [np.ascontiguousarray(th[i]) for i in range(r.n)]
+    for i, row in enumerate(keep):
+        fk.fake_set(blk, i, fk.fake_float_array(f, row.ctypes.data))
+    fk.fake_set(outer, 0, blk)
+    ptr32 = r.csr_ptr.astype(np.int32)
+    fn = A.lib.Java_org_apache_spark_ml_recommendation_CuMFJNIInterface_doALSWithCSR
+    fn.restype = ctypes.c_void_p
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.c_void_p, ctypes.c_void_p]
+    old = A.get_dropin_options()
+    try:
+        A.set_dropin_options(A.options(precision=A.PREC_BF16, solver=A.SOLVER_CG))
+        outs = []
+        for withhold in (1, 0):
+            A.lib.als_debug_withhold_first_row(withhold)
+            jrow = fk.fake_int_array(len(ptr32), ptr32.ctypes.data)
+            jcol = fk.fake_int_array(len(r.csr_col), r.csr_col.ctypes.data)
+            jval = fk.fake_float_array(len(r.csr_val), r.csr_val.ctypes.data)
+            outs.append(fn(fk.fake_env(), None, r.m, r.n, f, r.nnz, 0.05, outer, jrow, jcol, jval))
+            assert fk.fake_live_critical() == 0 and fk.fake_open_frames() == 0
+    finally:
+        A.lib.als_debug_withhold_first_row(0)
+        A.set_dropin_options(old)
+    assert not outs[0]
+    assert outs[1] and fk.fake_length(outs[1]) == r.m

@@ -192,3 +192,35 @@ def test_wide_rank_runs_on_the_warp_specialised_kernel():
     Xr, _ = O.half_step(r.csr_ptr, r.csr_col, r.csr_val, rnd(th, A.PREC_BF16), 0.05)
     keep = np.diff(r.csr_ptr) > 0
     assert rel_rows(X, Xr)[keep].max() < TOL
+
+
+def test_bounded_wait_gives_up_and_the_next_half_step_is_clean():
+    """The kernels' waits are bounded. A test switch makes the first CTA never
+    mark its first row's accumulator complete (a flag that nothing sets): that
+    row's solver gives up after its 2 s limit, every role leaves its loop, the
+    kernel returns with the error word set, and the host reads
+    kernel_errors == 1. No fault, no hang: the same model's next half-step
+    runs normally and matches the oracle."""
+    import time
+    r = A.synth(A.scaled_config("netflix", 0.03), seed=41)
+    f = 32
+    th = A.init_factors(r.n, f, 43)
+    M = A.Model(r, f, A.options(precision=A.PREC_BF16, solver=A.SOLVER_CG, warm_start=A.WARM_ZERO,
+                                solver_groups=2), theta0=th)
+    torch.cuda.synchronize()
+    assert A.lib.als_debug_withhold_first_row(1) == 0
+    t0 = time.time()
+    M.half_step(A.SIDE_USERS, 0.05)
+    torch.cuda.synchronize()
+    dt = time.time() - t0
+    st = M.stats(reset=True)
+    assert st["kernel_errors"] == 1, st
+    assert 1.5 < dt < 60, dt  # the wait ran to its limit, and no longer
+    M.half_step(A.SIDE_USERS, 0.05)
+    X = M.factors()[0].cpu().numpy()
+    st = M.stats()
+    M.close()
+    assert st["kernel_errors"] == 0 and st["rows_solved"] == r.m, st
+    Xr, _ = O.half_step(r.csr_ptr, r.csr_col, r.csr_val, rnd(th, A.PREC_BF16), 0.05)
+    keep = np.diff(r.csr_ptr) > 0
+    assert rel_rows(X, Xr)[keep].max() < TOL
