@@ -1,6 +1,6 @@
 """Row sharding across ranks: partition balance, and a 2-rank gloo run of the
-sharded iteration (each rank solves its rows, then rows are exchanged) that
-must equal the unsharded ALS. The per-rank solver here is a CPU stand-in
+sharded iteration (each rank solves its rows, then the rows are exchanged by
+one all-gather per half-step) that must equal the unsharded ALS. The per-rank solver here is a CPU stand-in
 built on the oracle; the exchange logic is the one the GPU ranks use."""
 import os
 import socket
@@ -25,6 +25,22 @@ def test_partition_balanced_and_contiguous():
             cost = np.diff(ptr) * 1e4 + 1e6 / 3
             shares = [cost[b[k]:b[k + 1]].sum() for k in range(world)]
             assert max(shares) <= cost.sum() / world + cost.max() + 1
+
+
+def test_gather_blocks_cover_every_range():
+    rng = np.random.default_rng(3)
+    cases = [np.array([0, 5, 5, 12]), np.array([0, 0, 7]), np.array([0, 9]),
+             np.array([0, 1, 2, 3, 40])]
+    for _ in range(50):
+        world = int(rng.integers(1, 9))
+        cuts = np.sort(rng.integers(0, 200, world - 1))
+        cases.append(np.concatenate([[0], cuts, [int(rng.integers(max(cuts.max(initial=0), 1), 300))]]))
+    for b in cases:
+        span, start = D.gather_blocks(b)
+        rows = b[-1]
+        assert span == np.diff(b).max()
+        for r in range(len(b) - 1):
+            assert 0 <= start[r] <= b[r] and b[r + 1] <= start[r] + span <= rows
 
 
 class CpuModel:
@@ -83,9 +99,10 @@ def _free_port():
     return p
 
 
-def test_two_rank_gloo_sharded_iteration_equals_unsharded(tmp_path):
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_sharded_iteration_equals_unsharded(tmp_path, world):
     out = str(tmp_path / "xt.npy")
-    mp.start_processes(_worker, args=(2, _free_port(), out), nprocs=2, join=True,
+    mp.start_processes(_worker, args=(world, _free_port(), out), nprocs=world, join=True,
                        start_method="spawn")
     got = np.load(out)
     r = A.synth(A.scaled_config("ml1m", 0.1), seed=4)
