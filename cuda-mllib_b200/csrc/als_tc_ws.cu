@@ -57,8 +57,6 @@ template <int NG> __host__ __device__ constexpr int threads() { return 128 * NG 
 template <int NG> __host__ __device__ constexpr int prod_warp() { return 4 * NG; }  // 4NG+2, 4NG+3 too
 template <int NG> __host__ __device__ constexpr int mma_warp() { return 4 * NG + 1; }
 constexpr int NS = 6;                             // shared-memory stages
-constexpr int KS = 64;                            // ratings per stage
-constexpr int kAtom = (KS / 8) * 1024;            // one 64-element MN atom of a stage
 constexpr int kMaxAcc = 4;                        // TMEM accumulators at most
 constexpr int kMaxGroups = 3;                     // solver warpgroups per CTA at most
 // Shape of an instance by its Cholesky tile extent FP (f <= FP): up to f = 112
@@ -68,10 +66,20 @@ constexpr int kMaxGroups = 3;                     // solver warpgroups per CTA a
 // reaches 144, so TMEM holds three accumulators of 160 columns; a 128-wide
 // Cholesky tile would need 136 tiles for 128 threads, so rows CG cannot finish
 // are handed to a post-pass of the one-CTA-per-row kernel.
+// Ratings per stage: every shared-memory operation of the MMA thread (its
+// barrier wait, the stage-info read, the commit) waits behind the MMAs it has
+// queued, so each stage's bookkeeping leaves the tensor pipe idle for roughly
+// the time of three to four 128 x 112 x 16 MMAs; 128-rating stages (eight MMAs
+// a stage) halve that per rating. The wide shape's three atoms keep 64-rating
+// stages so that six stages fit in shared memory.
 template <int FP> struct Dims {
   static constexpr bool kWide = FP > 112;
+  static constexpr int kKS = kWide ? 64 : 128;        // ratings per stage
+  static constexpr int kAtom = (kKS / 8) * 1024;      // one 64-element MN atom of a stage
   static constexpr int kAtoms = kWide ? 3 : 2;
   static constexpr int kStageBytes = kAtoms * kAtom;
+  static constexpr int kDI = kWide ? 8 : 5;           // index-ring slots (stages fetched ahead + 1)
+  static constexpr int kRingSlot = 8 * kKS + 48;      // column indices, ratings, three int4 of header
   static constexpr int kAcc = kWide ? 3 : 4;          // row n -> accumulator n mod kAcc
   static constexpr int kBufCols = kWide ? 160 : 128;  // TMEM columns per accumulator
   static constexpr bool kChol = !kWide;               // the in-kernel Cholesky fallback
@@ -100,9 +108,15 @@ template <int NG> __host__ __device__ constexpr unsigned row_parity(long long n)
 }
 constexpr int kTmemCols = 512;                    // allocated: all of TMEM
 constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
-constexpr int DI = 8;                             // index-ring slots (stages fetched ahead + 1)
-constexpr int kRingSlot = 8 * KS + 48;            // column indices, ratings, three int4 of header
 constexpr int kProducers = 3;                     // producer warps, taking stages in turn
+// Stage info word, written by the stage's producer before it arrives on the
+// stage's full barrier and read by the MMA thread in one load: accumulator
+// (bits 0-1), MMAs of K = 16 (bits 2-5), first and last stage of the row
+// (bits 6, 7); kInfoEnd marks the end of the CTA's stages.
+constexpr uint32_t kInfoEnd = 1u << 31;
+__host__ __device__ constexpr uint32_t stage_word(int acc, int kmma, int first, int last) {
+  return (uint32_t)acc | ((uint32_t)kmma << 2) | ((uint32_t)first << 6) | ((uint32_t)last << 7);
+}
 static_assert(NS % kProducers == 0, "a stage slot always belongs to the same producer");
 }  // namespace ws
 
@@ -140,8 +154,9 @@ struct WsLayoutT {
   static constexpr size_t kBars = 8 * (2 * ws::NS + 2 * ws::kMaxAcc + 2 * ws::kRowSlots + 2);
   static constexpr size_t kCtrl = kBars + 16 * (ws::NS + ws::kRowSlots) + 16;
   static constexpr size_t oRing = oCtrl + kCtrl;  // 16-byte aligned
-  static constexpr size_t kTotal = 1024 + oRing + (size_t)ws::kProducers * ws::DI * ws::kRingSlot;
-  static_assert(kCtrl % 16 == 0 && ws::kRingSlot % 16 == 0, "ring alignment");
+  static constexpr size_t kTotal =
+      1024 + oRing + (size_t)ws::kProducers * ws::Dims<FP>::kDI * ws::Dims<FP>::kRingSlot;
+  static_assert(kCtrl % 16 == 0 && ws::Dims<FP>::kRingSlot % 16 == 0, "ring alignment");
 };
 
 template <int FP, int NP, int NG>
@@ -151,7 +166,8 @@ using WsLayout = typename std::conditional<WsLayoutT<FP, NP, NG, true>::kTotal <
 
 struct WsCtrl {
   uint64_t *full, *empty, *acc_full, *acc_empty, *row_full, *row_empty, *drain;
-  int4 *stage_info, *row_info;
+  uint32_t *stage_info;  // one info word per stage slot
+  int4 *row_info;
   volatile int *misc;  // [0] TMEM base, [1] abort, [2] producer queue slot
 };
 
@@ -210,7 +226,7 @@ __device__ __forceinline__ void cp_async4(uint32_t dst, const void *src) {
 // indices and ratings of the stages it owns into its shared-memory ring with
 // cp.async (one commit group per owned stage). Rows without ratings are
 // finished by the cursor of producer 0 (x_u = 0).
-template <typename LP>
+template <typename LP, int KS>
 struct FetchCursor {
   ItemBatch cb, nb;
   long long bi;
@@ -275,7 +291,7 @@ struct FetchCursor {
                                           unsigned long long &n_empty) {
     if (u < 0) return;
     ++gs;
-    k0 += ws::KS;
+    k0 += KS;
     if (k0 >= e) {
       next_item(p, lane);
       settle(a, p, lane, n_empty);
@@ -286,21 +302,21 @@ struct FetchCursor {
   // part, heavy}, {kc, first, last, valid}, {row, stage}; past the end the
   // header is invalid and carries the number of rows and stages
   __device__ __forceinline__ void fetch(const RowsArgs &a, unsigned char *rs, int lane) {
-    int4 *h = reinterpret_cast<int4 *>(rs + 8 * ws::KS);
+    int4 *h = reinterpret_cast<int4 *>(rs + 8 * KS);
     if (u >= 0) {
-      const int kc = (int)(e - k0 < ws::KS ? e - k0 : ws::KS);
+      const int kc = (int)(e - k0 < KS ? e - k0 : KS);
       const uint32_t r0 = tc::smem_u32(rs);
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
+      for (int j = 0; j < KS / 32; ++j) {
         const int k = lane + 32 * j;
         if (k < kc) {
           cp_async4(r0 + 4 * k, a.col + k0 + k);
-          cp_async4(r0 + 4 * ws::KS + 4 * k, a.val + k0 + k);
+          cp_async4(r0 + 4 * KS + 4 * k, a.val + k0 + k);
         }
       }
       if (lane == 0) {
         h[0] = make_int4(u, deg, part, heavy);
-        h[1] = make_int4(kc, k0 == s ? 1 : 0, k0 + ws::KS >= e ? 1 : 0, 1);
+        h[1] = make_int4(kc, k0 == s ? 1 : 0, k0 + KS >= e ? 1 : 0, 1);
         h[2] = make_int4(row, gs, 0, 0);
       }
     } else if (lane == 0) {
@@ -311,35 +327,19 @@ struct FetchCursor {
   }
 };
 
-// One stage's factor rows: lanes 16h + j copy 16-byte piece j (< nj = ld / 8)
-// of rows k = 32h .. 32h + 31 (< krows) into the 128B-swizzled MN-major tile
-// (piece j of row k lands in atom j / 8, 8-row group k / 8, row k mod 8,
-// 16-byte chunk (j mod 8) xor (k mod 8)). Rows at or past kc are zero-filled;
-// a column index outside the factor matrix is clamped to its last row, so a
-// malformed CSR gives wrong numbers but never reads outside the factors. The
-// 32 column indices are read first, so the copies issue back to back.
-__device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &plan, int nj,
-                                             const int *cols, int kc, int krows, uint32_t sa,
-                                             int lane) {
-  if (nj > 16) {
-    // piece 16 (tile columns 128-135, atom 2, 16-byte chunk 0 xor (k mod 8)) of
-    // rows lane and lane + 32, for ranks f > 120
-    const char *src16 = reinterpret_cast<const char *>(a.src) + 16 * 16;
-    const unsigned row_bytes = (unsigned)a.ld_src * 2u, last = (unsigned)plan.src_rows - 1u;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int k = lane + 32 * h;
-      if (k < krows) {
-        const bool in = k < kc;
-        const unsigned c = in ? min((unsigned)cols[k], last) : 0u;
-        const uint32_t dst = sa + 2u * ws::kAtom + (uint32_t)((k >> 3) * 1024 + (k & 7) * 128) +
-                             ((uint32_t)(k & 7) << 4);
-        cp_async16_zfill(dst, in ? src16 + (size_t)c * row_bytes : src16, in ? 16u : 0u);
-      }
-    }
-  }
-  const int j = lane & 15, k0 = (lane >> 4) * 32;
-  if (j >= nj || k0 >= krows) return;
+// One stage's factor rows: in each block of 64 rows, lanes 16h + j copy
+// 16-byte piece j (< nj = ld / 8) of rows 32h .. 32h + 31 (< krows) into the
+// 128B-swizzled MN-major tile (piece j of row k lands in atom j / 8, 8-row
+// group k / 8, row k mod 8, 16-byte chunk (j mod 8) xor (k mod 8)). Rows at or
+// past kc are zero-filled; a column index outside the factor matrix is clamped
+// to its last row, so a malformed CSR gives wrong numbers but never reads
+// outside the factors. The 32 column indices of a block are read first, so its
+// copies issue back to back.
+template <int KS>
+__device__ __forceinline__ void gather_block(const RowsArgs &a, const WsPlan &plan, int j,
+                                             int k0, const int *cols, int kc, int krows,
+                                             uint32_t sa) {
+  constexpr int kAtom = (KS / 8) * 1024;
   int ci[32];
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
@@ -351,7 +351,7 @@ __device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &pl
   }
   const char *srcb = reinterpret_cast<const char *>(a.src) + 16 * j;
   const unsigned row_bytes = (unsigned)a.ld_src * 2u, last = (unsigned)plan.src_rows - 1u;
-  const uint32_t dj = sa + (uint32_t)(j >> 3) * ws::kAtom + (uint32_t)(k0 >> 3) * 1024;
+  const uint32_t dj = sa + (uint32_t)(j >> 3) * kAtom + (uint32_t)(k0 >> 3) * 1024;
   const uint32_t jx = (uint32_t)(j & 7) << 4;
   if (kc >= k0 + 32) {  // every row of this half carries a rating
 #pragma unroll
@@ -375,6 +375,31 @@ __device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &pl
   }
 }
 
+template <int KS>
+__device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &plan, int nj,
+                                             const int *cols, int kc, int krows, uint32_t sa,
+                                             int lane) {
+  constexpr int kAtom = (KS / 8) * 1024;
+  if (nj > 16) {
+    // piece 16 (tile columns 128-135, atom 2, 16-byte chunk 0 xor (k mod 8)) of
+    // rows lane, lane + 32, ..., for ranks f > 120
+    const char *src16 = reinterpret_cast<const char *>(a.src) + 16 * 16;
+    const unsigned row_bytes = (unsigned)a.ld_src * 2u, last = (unsigned)plan.src_rows - 1u;
+    for (int k = lane; k < krows; k += 32) {
+      const bool in = k < kc;
+      const unsigned c = in ? min((unsigned)cols[k], last) : 0u;
+      const uint32_t dst = sa + 2u * kAtom + (uint32_t)((k >> 3) * 1024 + (k & 7) * 128) +
+                           ((uint32_t)(k & 7) << 4);
+      cp_async16_zfill(dst, in ? src16 + (size_t)c * row_bytes : src16, in ? 16u : 0u);
+    }
+  }
+  const int j = lane & 15;
+  if (j >= nj) return;
+#pragma unroll 1
+  for (int k0 = (lane >> 4) * 32; k0 < krows; k0 += 64)
+    gather_block<KS>(a, plan, j, k0, cols, kc, krows, sa);
+}
+
 // Producer k of ws::kProducers owns global stages k, k + kProducers, ...;
 // stage t of the sequence goes to shared-memory stage t mod NS (the
 // (t / NS)-th phase of its barriers), row r to row slot and accumulator
@@ -387,24 +412,26 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
                            const WsCtrl &c, unsigned char *stages, unsigned char *ring, int k,
                            unsigned long long &n_empty_rows) {
   constexpr int P = ws::kProducers;
+  using D = ws::Dims<FP>;
+  constexpr int KS = D::kKS, DI = D::kDI;
   const int lane = threadIdx.x & 31;
   const uint32_t st0 = tc::smem_u32(stages);
-  FetchCursor<LP> fc;
+  FetchCursor<LP, KS> fc;
   fc.init(a, plan, lane, k == 0, n_empty_rows);
   for (int i = 0; i < k; ++i) fc.advance(a, plan, lane, n_empty_rows);
   auto fetch_next = [&](long long t) {
-    fc.fetch(a, ring + (int)(t % ws::DI) * ws::kRingSlot, lane);
+    fc.fetch(a, ring + (int)(t % DI) * D::kRingSlot, lane);
     for (int i = 0; i < P; ++i) fc.advance(a, plan, lane, n_empty_rows);
   };
-  for (int q = 0; q < ws::DI - 1; ++q) fetch_next(q);
+  for (int q = 0; q < DI - 1; ++q) fetch_next(q);
   bool ends = false;
   int end_rows = 0, end_stage = 0;
   for (long long t = 0;; ++t) {
-    fetch_next(t + ws::DI - 1);
-    asm volatile("cp.async.wait_group %0;" ::"n"(ws::DI - 1) : "memory");
+    fetch_next(t + DI - 1);
+    asm volatile("cp.async.wait_group %0;" ::"n"(DI - 1) : "memory");
     __syncwarp();
-    const unsigned char *rs = ring + (int)(t % ws::DI) * ws::kRingSlot;
-    const int4 *hd = reinterpret_cast<const int4 *>(rs + 8 * ws::KS);
+    const unsigned char *rs = ring + (int)(t % DI) * D::kRingSlot;
+    const int4 *hd = reinterpret_cast<const int4 *>(rs + 8 * KS);
     const int4 h1 = hd[1], h2 = hd[2];
     if (__any_sync(0xffffffffu, h1.w == 0 || c.misc[1] != 0)) {  // warp-uniform exit
       ends = h1.w == 0 && c.misc[1] == 0 && h2.y == (int)(P * t + k);
@@ -421,7 +448,7 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     }
     // every stage of row h2.x accumulates into accumulator h2.x mod kAcc, whichever
     // producer took the row's first stage
-    const int acc = (int)((unsigned)h2.x % (unsigned)ws::Dims<FP>::kAcc);
+    const int acc = (int)((unsigned)h2.x % (unsigned)D::kAcc);
     if (first) {
       // the row's first stage also hands row h2.x to its solver group
       const int r = h2.x, rs2 = ws::row_slot<NG>(r);
@@ -440,14 +467,14 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     if (st >= ws::NS)
       okw = tc::mbar_wait_or_abort(&c.empty[slot], (unsigned)((st / ws::NS) - 1) & 1u, c.misc + 1);
     if (!__all_sync(0xffffffffu, okw)) { c.misc[1] = 1; break; }
-    const uint32_t sa = st0 + (uint32_t)slot * ws::Dims<FP>::kStageBytes;
-    if (lane == 0) c.stage_info[slot] = make_int4(acc, krows / 16, first, last);
-    gather_stage(a, plan, g.nj, reinterpret_cast<const int *>(rs), kc, krows, sa, lane);
+    const uint32_t sa = st0 + (uint32_t)slot * D::kStageBytes;
+    if (lane == 0) c.stage_info[slot] = ws::stage_word(acc, krows / 16, first, last);
+    gather_stage<KS>(a, plan, g.nj, reinterpret_cast<const int *>(rs), kc, krows, sa, lane);
     // r_uk (0 past kc) into tile column c_r = 8 nj: atom c_r / 64, 16-byte
     // chunk ((c_r mod 64) / 8) xor (k mod 8), element 0; the chunk's other
     // elements stay zero
-    const float *vr = reinterpret_cast<const float *>(rs + 4 * ws::KS);
-    const uint32_t rbase = sa + (uint32_t)(g.nj >> 3) * ws::kAtom, rch = (uint32_t)(g.nj & 7);
+    const float *vr = reinterpret_cast<const float *>(rs + 4 * KS);
+    const uint32_t rbase = sa + (uint32_t)(g.nj >> 3) * D::kAtom, rch = (uint32_t)(g.nj & 7);
     for (int kk = lane; kk < krows; kk += 32) {
       const uint16_t w = kk < kc ? tc::to_bits<LP>(vr[kk]) : (uint16_t)0;
       const uint32_t dst = rbase + (kk >> 3) * 1024 + (kk & 7) * 128 + ((rch ^ (uint32_t)(kk & 7)) << 4);
@@ -465,7 +492,7 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
   if (end_stage >= ws::NS)
     tc::mbar_wait_or_abort(&c.empty[slot], (unsigned)((end_stage / ws::NS) - 1) & 1u, c.misc + 1);
   if (lane == 0) {
-    c.stage_info[slot] = make_int4(-1, 0, 0, 0);
+    c.stage_info[slot] = ws::kInfoEnd;
     mbar_arrive_cnt(&c.full[slot], ws::kFullCount);
     // end markers: rows end_rows .. end_rows + NG - 1, the next row of each solver warpgroup
     for (int i = 0; i < NG; ++i) {
@@ -488,9 +515,11 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
                        uint32_t idesc, bool withhold_first) {
   // (test support: with withhold_first, the first item's accumulator is never
   // marked full, so its solver's bounded wait runs out)
+  using D = ws::Dims<FP>;
   long long items_done = 0;
-  const uint32_t lbo = (ws::KS / 8) * 1024, sbo = 1024;
-  const uint32_t st0 = tc::smem_u32(stages);
+  // descriptors by addition: the start-address field (bits 0-13, address / 16)
+  // of stage slot s, K step kk is that of slot 0 plus (s * stage + kk * 2 KB) / 16
+  const uint64_t desc0 = tc::make_desc(tc::smem_u32(stages), D::kAtom, 1024);
   unsigned full_par = 0, acc_used = 0, acc_par = 0;
   int slot = 0;
   bool ok = true;
@@ -498,10 +527,10 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
     ok = tc::mbar_wait_or_abort(&c.full[slot], (full_par >> slot) & 1, c.misc + 1);
     if (!ok) break;
     full_par ^= 1u << slot;
-    const volatile int *vi = reinterpret_cast<volatile int *>(&c.stage_info[slot]);
-    const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
-    if (info.x < 0) break;
-    const int b = info.x, kmma = info.y, first = info.z, last = info.w;
+    const uint32_t info = *reinterpret_cast<const volatile uint32_t *>(&c.stage_info[slot]);
+    if (info & ws::kInfoEnd) break;
+    const int b = (int)(info & 3u), kmma = (int)((info >> 2) & 15u), first = (int)((info >> 6) & 1u),
+              last = (int)((info >> 7) & 1u);
     // No proxy fence here: each producer lane fences its own generic stores of
     // the ratings before arriving, and the cp.async copies reach the barrier
     // only once they have landed (the pattern CUTLASS's sm100 cp.async
@@ -515,11 +544,11 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
       acc_used |= 1u << b;
     }
     tc::tc_fence_after();
-    const uint32_t sa = st0 + (uint32_t)slot * ws::Dims<FP>::kStageBytes;
+    const uint64_t ds = desc0 + (uint64_t)(((uint32_t)slot * D::kStageBytes) >> 4);
+    const uint32_t td = tmem + (uint32_t)b * D::kBufCols;
     for (int kk = 0; kk < kmma; ++kk) {
-      const uint64_t desc = tc::make_desc(sa + kk * 2 * sbo, lbo, sbo);
-      tc::mma_f16(tmem + (uint32_t)b * ws::Dims<FP>::kBufCols, desc, desc, idesc,
-                  (first && kk == 0) ? 0u : 1u);
+      const uint64_t desc = ds + (uint64_t)(kk * (2048 >> 4));
+      tc::mma_f16(td, desc, desc, idesc, (first && kk == 0) ? 0u : 1u);
     }
     tc::mma_commit(&c.empty[slot]);
     if (last) {
@@ -1444,8 +1473,8 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
   c.row_full = c.acc_empty + ws::kMaxAcc;
   c.row_empty = c.row_full + ws::kRowSlots;
   c.drain = c.row_empty + ws::kRowSlots;
-  c.stage_info = reinterpret_cast<int4 *>(ctrl + L::kBars);
-  c.row_info = c.stage_info + ws::NS;
+  c.stage_info = reinterpret_cast<uint32_t *>(ctrl + L::kBars);
+  c.row_info = reinterpret_cast<int4 *>(ctrl + L::kBars) + ws::NS;
   c.misc = reinterpret_cast<volatile int *>(c.row_info + ws::kRowSlots);
   const int tid = threadIdx.x, warp = tid >> 5;
   const WsPlan &plan = plan_arg;  // stays in the parameter space
@@ -1487,8 +1516,9 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
     __syncwarp();
   } else if (warp == ws::prod_warp<NG>() || warp >= ws::prod_warp<NG>() + 2) {
     const int k = warp == ws::prod_warp<NG>() ? 0 : warp - ws::prod_warp<NG>() - 1;
-    ws_produce<FP, LP, NG>(a, plan, g, c, base, base + L::oRing + (size_t)k * ws::DI * ws::kRingSlot, k,
-                       n_empty);
+    ws_produce<FP, LP, NG>(a, plan, g, c, base,
+                           base + L::oRing + (size_t)k * ws::Dims<FP>::kDI * ws::Dims<FP>::kRingSlot,
+                           k, n_empty);
     if ((tid & 31) == 0 && a.counters && n_empty) atomicAdd(&a.counters->rows, n_empty);
   } else if (warp < 4 * NG) {
     unsigned char *mem = base + L::oSolver + (size_t)(warp >> 2) * L::kSolver;
