@@ -84,27 +84,35 @@ template <int FP> struct Dims {
   static constexpr int kBufCols = kWide ? 160 : 128;  // TMEM columns per accumulator
   static constexpr bool kChol = !kWide;               // the in-kernel Cholesky fallback
 };
-// Row hand-over slots: kGroupSlots per solver warpgroup. Row n goes to group
-// n mod NG, the k-th row of a group (k = n / NG) to its slot k mod
-// kGroupSlots, as that slot's (k / kGroupSlots)-th barrier phase. An mbarrier
-// parity wait tells only the current and the preceding phase apart, so no
-// wait may name a phase two ahead of its barrier's:
-//  - a group waits only on its own slots, in its own order;
-//  - a producer posting row r waits for the slot's previous row, r - 8 NG,
-//    to have been taken. When it posts row r it has finished its previous
-//    stage, (first stage of r) - P with P producers, whose slot wait means
-//    the MMA has issued stage (first stage of r) - P - NS and so acquired
-//    the accumulator of its row R' >= r - P - NS; every row up to
+// Row hand-over: the solver warpgroups claim the CTA's rows in order from a
+// shared counter, each taking the next row when it is free. (With a fixed
+// assignment, row n to group n mod NG, a group's next row n + NG reuses the
+// accumulator of row n + NG - kAcc, which another group may still hold.) Row
+// n is posted in slot n mod kRowSlots, as that slot's (n / kRowSlots)-th
+// barrier phase. An mbarrier parity wait tells only the current and the
+// preceding phase apart, so no wait may name a phase two ahead of its
+// barrier's:
+//  - rows are claimed in order and a group claims a row only after taking
+//    and finishing its previous one, so at most NG rows are claimed and not
+//    yet taken: row n - kRowSlots has been taken before any group waits for
+//    row n;
+//  - a group waits for row n's accumulator (its (n / kAcc)-th fill) only
+//    once fill n / kAcc - 1, by row n - kAcc, is complete: of the kAcc rows
+//    n - kAcc .. n - 1 the other NG - 1 < kAcc groups hold at most NG - 1
+//    unfinished, so one of them has been finished, its accumulator seen
+//    full, and the MMA fills rows in order;
+//  - a producer posting row r waits for the slot's previous row,
+//    r - kRowSlots, to have been taken. When it posts row r it has finished
+//    its previous stage, (first stage of r) - P with P producers, whose slot
+//    wait means the MMA has issued stage (first stage of r) - P - NS and so
+//    acquired the accumulator of its row R' >= r - P - NS; every row up to
 //    R' - kAcc >= r - P - NS - kAcc >= r - 13 has then handed its
-//    accumulator back, so it has been taken, and r - 16 NG (two slot uses
-//    back) is among them.
-constexpr int kGroupSlots = 8;
-constexpr int kRowSlots = kGroupSlots * kMaxGroups;
-template <int NG> __host__ __device__ constexpr int row_slot(long long n) {
-  return (int)(n % NG) * kGroupSlots + (int)((n / NG) % kGroupSlots);
-}
-template <int NG> __host__ __device__ constexpr unsigned row_parity(long long n) {
-  return (unsigned)((n / NG) / kGroupSlots) & 1u;
+//    accumulator back, so it has been taken, and r - 2 kRowSlots (two slot
+//    uses back) is among them.
+constexpr int kRowSlots = 24;
+__host__ __device__ constexpr int row_slot(long long n) { return (int)(n % kRowSlots); }
+__host__ __device__ constexpr unsigned row_parity(long long n) {
+  return (unsigned)(n / kRowSlots) & 1u;
 }
 constexpr int kTmemCols = 512;                    // allocated: all of TMEM
 constexpr int kFullCount = 33;                    // 32 cp.async arrivals + the rating-store arrive
@@ -168,7 +176,7 @@ struct WsCtrl {
   uint64_t *full, *empty, *acc_full, *acc_empty, *row_full, *row_empty, *drain;
   uint32_t *stage_info;  // one info word per stage slot
   int4 *row_info;
-  volatile int *misc;  // [0] TMEM base, [1] abort, [2] producer queue slot
+  volatile int *misc;  // [0] TMEM base, [1] abort, [2] producer queue slot, [3] rows claimed
 };
 
 __device__ __forceinline__ void ws_abort(const RowsArgs &a, const WsCtrl &c) {
@@ -403,7 +411,7 @@ __device__ __forceinline__ void gather_stage(const RowsArgs &a, const WsPlan &pl
 // Producer k of ws::kProducers owns global stages k, k + kProducers, ...;
 // stage t of the sequence goes to shared-memory stage t mod NS (the
 // (t / NS)-th phase of its barriers), row r to row slot and accumulator
-// r mod kAcc and to row slot row_slot<NG>(r), so the producers need no
+// r mod kAcc and to row slot row_slot(r), so the producers need no
 // coordination beyond those barriers.
 // The producer that owns the stage just past the last one writes the end
 // markers.
@@ -451,12 +459,12 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     const int acc = (int)((unsigned)h2.x % (unsigned)D::kAcc);
     if (first) {
       // the row's first stage also hands row h2.x to its solver group
-      const int r = h2.x, rs2 = ws::row_slot<NG>(r);
+      const int r = h2.x, rs2 = ws::row_slot(r);
       if (lane == 0) {
         bool okr = true;
-        if (r >= ws::kGroupSlots * NG)  // the slot's previous row has been taken
-          okr = tc::mbar_wait_or_abort(&c.row_empty[rs2],
-                                       ws::row_parity<NG>(r - ws::kGroupSlots * NG), c.misc + 1);
+        if (r >= ws::kRowSlots)  // the slot's previous row has been taken
+          okr = tc::mbar_wait_or_abort(&c.row_empty[rs2], ws::row_parity(r - ws::kRowSlots),
+                                       c.misc + 1);
         if (!okr) c.misc[1] = 1;
         c.row_info[rs2] = hd[0];
         tc::mbar_arrive(&c.row_full[rs2]);
@@ -496,10 +504,9 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
     mbar_arrive_cnt(&c.full[slot], ws::kFullCount);
     // end markers: rows end_rows .. end_rows + NG - 1, the next row of each solver warpgroup
     for (int i = 0; i < NG; ++i) {
-      const int r = end_rows + i, bb = ws::row_slot<NG>(r);
-      if (r >= ws::kGroupSlots * NG)
-        tc::mbar_wait_or_abort(&c.row_empty[bb], ws::row_parity<NG>(r - ws::kGroupSlots * NG),
-                               c.misc + 1);
+      const int r = end_rows + i, bb = ws::row_slot(r);
+      if (r >= ws::kRowSlots)
+        tc::mbar_wait_or_abort(&c.row_empty[bb], ws::row_parity(r - ws::kRowSlots), c.misc + 1);
       c.row_info[bb] = make_int4(-1, 0, 0, 0);
       tc::mbar_arrive(&c.row_full[bb]);
     }
@@ -513,8 +520,9 @@ __device__ void ws_produce(const RowsArgs &a, const WsPlan &plan, const WsGeom &
 template <int FP>
 __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages, uint32_t tmem,
                        uint32_t idesc, bool withhold_first) {
-  // (test support: with withhold_first, the first item's accumulator is never
-  // marked full, so its solver's bounded wait runs out)
+  // (test support: with withhold_first the issuer stops after the first item's
+  // MMAs without marking its accumulator full, as an issuer that stalls would,
+  // so the solvers' and producers' bounded waits run out)
   using D = ws::Dims<FP>;
   long long items_done = 0;
   // descriptors by addition: the start-address field (bits 0-13, address / 16)
@@ -552,7 +560,8 @@ __device__ void ws_mma(const RowsArgs &a, const WsCtrl &c, unsigned char *stages
     }
     tc::mma_commit(&c.empty[slot]);
     if (last) {
-      if (!(withhold_first && items_done == 0)) tc::mma_commit(&c.acc_full[b]);
+      if (withhold_first && items_done == 0) break;
+      tc::mma_commit(&c.acc_full[b]);
       ++items_done;
     }
     slot = slot + 1 == ws::NS ? 0 : slot + 1;
@@ -700,10 +709,11 @@ __device__ __forceinline__ float4 group_sum4(float4 v, float *red, int &slot, co
   return t;
 }
 
-// Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA. Row n
-// arrives in row slot row_slot<NG>(n) and accumulator n mod kAcc (the
-// (n / kAcc)-th phase of its barriers); the group keeps the accumulator until the row is solved:
-// the CG matrix-vector products read A_u from TMEM.
+// Solver warpgroup wg of NG claims the CTA's rows in order (the next one each
+// time it is free). Row n arrives in row slot row_slot(n) and accumulator
+// n mod kAcc (the (n / kAcc)-th phase of its barriers); the group keeps the
+// accumulator until the row is solved: the CG matrix-vector products read A_u
+// from TMEM.
 template <int FP, int NP, typename LP, int NG>
 __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &sv,
                          const WsCtrl &c, unsigned char *mem, uint32_t tmem, int wg) {
@@ -730,16 +740,21 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
   const uint32_t tlane = tmem + ((uint32_t)(wl * 32) << 16);
   const uint32_t bcol = (uint32_t)(a.ld_src & ~15);
   const int bq = a.ld_src & 15;
-  for (long long n = wg;; n += NG) {
-    const int rb = ws::row_slot<NG>(n), ab = (int)(n & (ws::Dims<FP>::kAcc - 1));
+  volatile int *claim = bad + 3;  // the row this group claimed last
+  for (;;) {
+    // the next row of the CTA; the barrier also ends every read of the
+    // previous row's broadcast vector
+    if (lt == 0) *claim = atomicAdd(const_cast<int *>(c.misc + 3), 1);
+    B.sync();
+    const long long n = *claim;
+    const int rb = ws::row_slot(n), ab = (int)(n & (ws::Dims<FP>::kAcc - 1));
     const unsigned par = (unsigned)(n / ws::Dims<FP>::kAcc) & 1u;
     const uint32_t tA = tlane + (uint32_t)ab * ws::Dims<FP>::kBufCols;
-    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], ws::row_parity<NG>(n), c.misc + 1);
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], ws::row_parity(n), c.misc + 1);
     if (!B.all(ok)) { ws_abort(a, c); break; }
     const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[rb]);
     const int4 info = make_int4(vi[0], vi[1], vi[2], vi[3]);
-    B.sync();
-    if (lt == 0) tc::mbar_arrive(&c.row_empty[rb]);
+    tc::mbar_arrive(&c.row_empty[rb]);  // every thread, once it has read the slot
     if (info.x < 0) break;
     const int64_t u = info.x;
     const float reg = a.lambda * (float)info.y;
@@ -889,9 +904,9 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
         flags |= kRowCgFallback;
         if (lt == 0) ++n_fb;
       }
-      B.sync();
     }
     if (!solved) {
+      B.sync();  // the last reduction has been read: its slots and the tile are free
       // the system into shared memory for the register-tile Cholesky
 #pragma unroll
       for (int c0 = 0; c0 < NP; c0 += 16) {
@@ -1171,9 +1186,9 @@ struct RowSystem<KA, false> {
   }
 };
 
-// Solver warpgroup wg of NG takes rows n = wg, wg + NG, ... of its CTA. Row n
-// arrives in row slot row_slot<NG>(n) and accumulator n mod kAcc (the
-// (n / kAcc)-th phase of its barriers). CG (optionally Jacobi-preconditioned)
+// Solver warpgroup wg of NG claims the CTA's rows in order (the next one each
+// time it is free). Row n arrives in row slot row_slot(n) and accumulator
+// n mod kAcc (the (n / kAcc)-th phase of its barriers). CG (optionally Jacobi-preconditioned)
 // from the warm start scaled optimally along itself, to relative residual
 // cg_tol in at most cg_max_steps steps; a reduction is written as partial sums
 // before its barrier and read after it, and the barriers that publish the
@@ -1221,20 +1236,24 @@ __device__ void ws_solve_wide(const RowsArgs &a, const WsPlan &plan, const TcSol
   const uint32_t bcol = (uint32_t)(a.ld_src & ~15);
   const int bq = a.ld_src & 15;
   const bool cg = sv.solver == 1;
-  for (long long n = wg;; n += NG) {
-    const int rb = ws::row_slot<NG>(n);
+  volatile int *claim = bad + 3;  // the row this group claimed last
+  for (;;) {
+    // the next row of the CTA
+    if (lt == 0) *claim = atomicAdd(const_cast<int *>(c.misc + 3), 1);
+    B.sync();
+    const long long n = *claim;
+    const int rb = ws::row_slot(n);
     const int ab = (int)((unsigned long long)n % (unsigned)D::kAcc);
     const unsigned par = (unsigned)((unsigned long long)n / (unsigned)D::kAcc) & 1u;
     const uint32_t tA = tlane + (uint32_t)ab * D::kBufCols;
-    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], ws::row_parity<NG>(n), c.misc + 1);
+    bool ok = tc::mbar_wait_or_abort(&c.row_full[rb], ws::row_parity(n), c.misc + 1);
     int4 info = make_int4(-1, 0, 0, 0);
     if (ok) {
       const volatile int *vi = reinterpret_cast<volatile int *>(&c.row_info[rb]);
       info = make_int4(vi[0], vi[1], vi[2], vi[3]);
+      tc::mbar_arrive(&c.row_empty[rb]);  // every thread, once it has read the slot
     }
-    // every thread has read the slot once all have passed this barrier
     if (!B.all(ok)) { ws_abort(a, c); break; }
-    if (lt == 0) tc::mbar_arrive(&c.row_empty[rb]);
     if (info.x < 0) break;
     const int64_t u = info.x;
     const float reg = a.lambda * (float)info.y;
@@ -1490,10 +1509,11 @@ rows_tc_ws_kernel(RowsArgs a, uint32_t idesc, TcSolve sv, WsGeom g, WsPlan plan_
     }
     for (int b = 0; b < ws::kRowSlots; ++b) {
       tc::mbar_init(&c.row_full[b], 1);
-      tc::mbar_init(&c.row_empty[b], 1);
+      tc::mbar_init(&c.row_empty[b], 128);  // every thread of the taking group
     }
     tc::mbar_init(c.drain, 1);
     c.misc[1] = 0;
+    c.misc[3] = 0;  // rows claimed by the solver warpgroups
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == ws::mma_warp<NG>()) {

@@ -280,13 +280,14 @@ int als_features(int64_t m, int32_t f, const int64_t *d_row_ptr, const int32_t *
                  void *d_features, int32_t ldf, cudaStream_t stream);
 
 /* Test support for the kernels' bounded waits: arms a one-shot fault for the
- * next tensor-core half-step (ranks 16..128 with a work plan): its first CTA
- * never marks the accumulator of its first row complete, so that row's solver
- * gives up its bounded wait (2 s), every role of the kernel leaves its loop,
- * the kernel returns with its error word set (als_stats.kernel_errors == 1)
- * and the half-step's results are incomplete; doALSWithCSR throws. Nothing
- * faults or hangs, and the next half-step runs normally. 0 disarms. No
- * counterpart in the reference. */
+ * next tensor-core half-step (ranks 16..128 with a work plan): the MMA issuer
+ * of its first CTA stops after its first row, without marking that row's
+ * accumulator complete, as a stalled issuer would. The waits of that CTA's
+ * solvers and producers give up (2 s), every role of the kernel leaves its
+ * loop, the kernel returns with its error word set
+ * (als_stats.kernel_errors == 1) and the half-step's results are incomplete;
+ * doALSWithCSR throws. Nothing faults or hangs, and the next half-step runs
+ * normally. 0 disarms. No counterpart in the reference. */
 int als_debug_withhold_first_row(int32_t enable);
 
 /* ---------------- 3. full training on host buffers ---------------- */

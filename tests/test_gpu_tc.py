@@ -195,12 +195,13 @@ def test_wide_rank_runs_on_the_warp_specialised_kernel():
 
 
 def test_bounded_wait_gives_up_and_the_next_half_step_is_clean():
-    """The kernels' waits are bounded. A test switch makes the first CTA never
-    mark its first row's accumulator complete (a flag that nothing sets): that
-    row's solver gives up after its 2 s limit, every role leaves its loop, the
-    kernel returns with the error word set, and the host reads
-    kernel_errors == 1. No fault, no hang: the same model's next half-step
-    runs normally and matches the oracle."""
+    """The kernels' waits are bounded. A test switch makes the first CTA's MMA
+    issuer stop after its first row without marking that row's accumulator
+    complete (a flag that nothing sets): the solvers and producers waiting on
+    it give up after their 2 s limit, every role leaves its loop, the kernel
+    returns with the error word set, and the host reads kernel_errors == 1.
+    No fault, no hang: the same model's next half-step runs normally and
+    matches the oracle."""
     import time
     r = A.synth(A.scaled_config("netflix", 0.03), seed=41)
     f = 32
