@@ -98,7 +98,8 @@ struct Side {
 // Dispatch one half-step: rows of `s` solved against factor `src`.
 cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, const float *src32,
                      int ld_src32, const void *src_lp, int ld_lp, float *dst32, void *dst_lp,
-                     Counters *ctr, const float *x0, int num_sms, cudaStream_t st) {
+                     Counters *ctr, const float *x0, bool learned_x0, int num_sms,
+                     cudaStream_t st) {
   if (s.active <= 0) return cudaSuccess;
   RowsArgs a{};
   a.m = s.active;
@@ -128,7 +129,8 @@ cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, c
   a.src = src_lp;
   a.ld_src = ld_lp;
   return launch_rows_tc(a, kind, o.solver, o.cg_max_steps, o.cg_tol, o.cg_jacobi,
-                        o.solver_groups, x0, s.has_plan ? &s.plan : nullptr, num_sms, st);
+                        o.solver_groups, x0, learned_x0 ? 1 : 0, s.has_plan ? &s.plan : nullptr,
+                        num_sms, st);
 }
 
 }  // namespace
@@ -408,8 +410,11 @@ static cudaError_t model_half(als_model *M, int side, float lambda, cudaStream_t
   }
   cudaError_t e;
   if (timing && (e = cudaEventRecord(M->tev[0], st)) != cudaSuccess) return e;
+  // a learned start is scaled optimally along itself before CG; the previous
+  // iterate is used as it is
+  const bool learned = M->opt.warm_start == ALS_WARM_MLP && !train;
   e = run_rows(S, M->f, lambda, o, src32, M->f, src_lp, M->lp_ld, dst32, dst_lp, M->ctr, x0,
-               M->num_sms, st);
+               learned, M->num_sms, st);
   if (e != cudaSuccess) return e;
   if (timing) {
     float ms = 0.f;
@@ -1132,7 +1137,7 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
       S.has_plan = true;
     }
     DROPIN_CALL(run_rows(S, f, lambda, o, (const float *)(d + oT), f, d + oL, ldp, (float *)(d + oX),
-                         nullptr, ctr, nullptr, sms, st),
+                         nullptr, ctr, nullptr, false, sms, st),
                 "doALSWithCSR: tensor-core half-step");
     DROPIN_CALL(cudaMemcpyAsync(&kernel_error, &ctr->error, sizeof(int), cudaMemcpyDeviceToHost, st),
                 "doALSWithCSR: error word");

@@ -19,10 +19,11 @@ cudaError_t launch_rows_fp32(const RowsArgs &a, int lp_kind, int num_sms, cudaSt
 bool tc_supported(int f);
 int tc_padded_ld(int f);  // row stride (elements) of the low-precision factor copy
 struct WsPlan;
-// x0: CG starting points (rows of stride a.ld_dst), or null.
+// x0: CG starting points (rows of stride a.ld_dst), or null; scale_x0: scale
+// each start optimally along itself before CG (for a learned start).
 cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
                            float cg_tol, int cg_jacobi, int groups, const float *x0,
-                           const WsPlan *plan, int num_sms, cudaStream_t st);
+                           int scale_x0, const WsPlan *plan, int num_sms, cudaStream_t st);
 
 // Solver parameters of one launch.
 struct TcSolve {
@@ -31,6 +32,7 @@ struct TcSolve {
   float cg_tol2;       // squared relative residual target
   const float *x0;     // CG starting point (m x ld_x0), or null for zero
   int ld_x0;
+  int scale_x0;        // 1: scale x0 optimally along itself first (a learned start)
   int jacobi;          // 1: diagonal preconditioner
   int groups;          // solver warpgroups per CTA of the warp-specialised kernel (1, 2 or 3)
   int prepare;         // 1: only load the kernel instance and set its attributes

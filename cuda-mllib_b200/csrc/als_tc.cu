@@ -283,7 +283,7 @@ rows_tc_kernel(RowsArgs a, TcGeom g, uint32_t idesc, TcSolve sv) {
         q = fmaf(arow[k + 2], p4.z, q);
         q = fmaf(arow[k + 3], p4.w, q);
       }
-      if (sv.x0) {
+      if (sv.scale_x0) {
         // Scale the warm start along its own direction: alpha = x0.b / x0.A x0
         // minimises the A-norm error of alpha * x0, so no start is worse than zero.
         const float xb = cta_sum<NT>(x * bm, red, rslot);
@@ -447,12 +447,12 @@ static cudaError_t launch_tc_np(const RowsArgs &a, int lp_kind, const TcSolve &s
 
 cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_max_steps,
                            float cg_tol, int cg_jacobi, int groups, const float *x0,
-                           const WsPlan *plan, int num_sms, cudaStream_t st) {
+                           int scale_x0, const WsPlan *plan, int num_sms, cudaStream_t st) {
   if (!tc_supported(a.f)) return cudaErrorNotSupported;
   if (a.ld_src != tc_padded_ld(a.f) || !a.error) return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(a.src) & 15) != 0) return cudaErrorInvalidValue;
-  TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst, cg_jacobi,
-             groups >= 1 && groups <= 3 ? groups : 2, 0, 0u};
+  TcSolve sv{solver, cg_max_steps, cg_tol * cg_tol, x0, a.ld_dst, x0 && scale_x0 ? 1 : 0,
+             cg_jacobi, groups >= 1 && groups <= 3 ? groups : 2, 0, 0u};
   RowsArgs ap = a;
   if (plan && tc_ws_takes(a.f, solver, cg_jacobi)) {
     const bool post = a.f > 112;

@@ -850,18 +850,25 @@ __device__ void ws_solve(const RowsArgs &a, const WsPlan &plan, const TcSolve &s
       if (!isfinite(x)) x = 0.f;
       float r = bm;
       if (sv.x0) {
-        // Scale the warm start optimally along its own direction:
-        // alpha = x0.b / x0.A x0 minimises the A-norm error of alpha * x0, so
-        // the start is never worse than zero in that norm.
-        ps[m] = x;
+        // r = b - A x0. A learned start is first scaled optimally along its
+        // own direction: alpha = x0.b / x0.A x0 minimises the A-norm error of
+        // alpha * x0, so the start is never worse than zero in that norm. The
+        // previous iterate is taken as it is (scaled, it needed more steps).
+        // x0 is broadcast in the second quarter of ps, so the first can take
+        // z while other threads still read x0.
+        ps[128 + m] = x;
         B.sync();
-        float q0 = matvec_tmem_np<NP>(tA, ps, reg, x);
+        float q0 = matvec_tmem_np<NP>(tA, ps + 128, reg, x);
         if (!live) q0 = 0.f;
-        const float2 xs = group_sum2(x * bm, x * q0, red, rslot, B);
-        float sc = xs.x / xs.y;
-        if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
-        x *= sc;
-        r = bm - sc * q0;
+        if (sv.scale_x0) {
+          const float2 xs = group_sum2(x * bm, x * q0, red, rslot, B);
+          float sc = xs.x / xs.y;
+          if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
+          x *= sc;
+          r = bm - sc * q0;
+        } else {
+          r = bm - q0;
+        }
       }
       if (!live) r = 0.f;
       float z = dinv * r;
@@ -1348,20 +1355,25 @@ __device__ void ws_solve_wide(const RowsArgs &a, const WsPlan &plan, const TcSol
       }
       float r = bm;
       if (sv.x0) {
-        // Scale the warm start optimally along its own direction:
-        // alpha = x0.b / x0.A x0 minimises the A-norm error of alpha * x0, so
-        // the start is never worse than zero in that norm. x0 was published
-        // with the accumulator vote (or after the split row's sums).
+        // r = b - A x0. A learned start is first scaled optimally along its
+        // own direction: alpha = x0.b / x0.A x0 minimises the A-norm error of
+        // alpha * x0, so the start is never worse than zero in that norm; the
+        // previous iterate is taken as it is. x0 was published with the
+        // accumulator vote (or after the split row's sums).
         float q0 = sys.mv(pv + ((ph - 1) & 1) * 256, reg, x);
         if (!live) q0 = 0.f;
-        group_partial2(x * bm, x * q0, rbuf(), lt);
-        B.sync();
-        const float2 xs = group_read2(rbuf());
-        ++ph;
-        float sc = xs.x / xs.y;
-        if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
-        x *= sc;
-        r = bm - sc * q0;
+        if (sv.scale_x0) {
+          group_partial2(x * bm, x * q0, rbuf(), lt);
+          B.sync();
+          const float2 xs = group_read2(rbuf());
+          ++ph;
+          float sc = xs.x / xs.y;
+          if (!(sc > 0.f) || !isfinite(sc)) sc = 0.f;
+          x *= sc;
+          r = bm - sc * q0;
+        } else {
+          r = bm - q0;
+        }
       }
       if (!live) r = 0.f;
       float z = dinv * r;
