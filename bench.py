@@ -14,7 +14,8 @@ Reference arm: the reference has no CPU ALS (its CPU path is Spark's JVM ALS,
 absent here), so it times the CPU port of the same half-step (oracle FP32) on
 bounded seeded row samples with all host threads, scaled by the formula.
 With N > 1 ranks, rows are sharded by nnz and each half-step ends with an
-all-gather of the updated factor rows (NCCL).
+all-gather of the updated factor rows: the engine's C++ shard driver
+(als_shard_*, NCCL), its communicator id handed out over torch.distributed.
 """
 import argparse
 import json
@@ -302,9 +303,12 @@ def run_engine(args):
         model = A.Model(r, f, opts, stream=stream, theta0=th0)
     shard = None
     if world > 1:
-        from als_dist import ShardedIteration
-        shard = ShardedIteration(model, r, world, rank, stream)
-        shard.apply()
+        import torch.distributed as dist
+        nid = torch.zeros(128, dtype=torch.uint8, device=dev)
+        if rank == 0:
+            nid.copy_(torch.frombuffer(bytearray(A.shard_unique_id()), dtype=torch.uint8))
+        dist.broadcast(nid, 0)
+        shard = A.Shard(model, r, world, rank, bytes(nid.cpu().tolist()))
 
     def restart(M):
         # a fresh training run: theta0 and X = 0, as a newly created model has
@@ -322,12 +326,12 @@ def run_engine(args):
             return
         M.half_step(A.SIDE_USERS, lam)
         if shard and M is model:
-            shard.gather(A.SIDE_USERS)
+            shard.exchange(A.SIDE_USERS)
         if ev is not None:
             ev[1].record(stream)
         M.half_step(A.SIDE_ITEMS, lam)
         if shard and M is model:
-            shard.gather(A.SIDE_ITEMS)
+            shard.exchange(A.SIDE_ITEMS)
         if ev is not None:
             ev[2].record(stream)
 
@@ -549,6 +553,8 @@ def run_engine(args):
                                           f"({frac:.2%}) of the same matrix, FP32 port, one pass"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if shard:
+        shard.close()  # collective: every rank destroys the communicator
     model.close()
     if world > 1:
         import torch.distributed as dist

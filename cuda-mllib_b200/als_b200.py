@@ -118,6 +118,17 @@ _sig(lib.als_set_dropin_options, c_i32, c_vp)
 _sig(lib.als_debug_withhold_first_row, c_i32, c_i32)
 _sig(lib.als_get_dropin_options, c_i32, c_vp)
 # mallocBest / freeBest keep the reference's C++ linkage; these are their C names
+_sig(lib.als_shard_unique_id, c_i32, c_vp)
+_sig(lib.als_shard_partition, c_i32, c_vp, c_i64, c_i32, c_i32, c_vp)
+_sig(lib.als_shard_blocks, c_i32, c_vp, c_i32, c_vp, c_vp)
+_sig(lib.als_shard_create, c_i32, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i32, c_i32, c_i32, c_vp,
+     c_vp)
+_sig(lib.als_shard_bounds, c_i32, c_vp, c_i32, c_vp)
+_sig(lib.als_shard_exchange, c_i32, c_vp, c_i32, c_vp)
+_sig(lib.als_shard_half_step, c_i32, c_vp, c_i32, c_f32, c_vp)
+_sig(lib.als_shard_iterate, c_i32, c_vp, c_f32, c_i32, c_vp)
+_sig(lib.als_shard_rmse, c_i32, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp)
+_sig(lib.als_shard_destroy, None, c_vp)
 _sig(lib.als_malloc_best, ctypes.c_int, c_vp, c_sz)
 _sig(lib.als_free_best, ctypes.c_int, c_vp)
 _sig(lib.get_gpu, ctypes.c_int)
@@ -278,6 +289,77 @@ class Model:
         _check(lib.als_model_rmse(self.handle, len(u), _ptr(u), _ptr(i), _ptr(r),
                                   ctypes.byref(out), self.stream))
         return float(out.value)
+
+
+def shard_partition(ptr, world: int, f: int) -> np.ndarray:
+    """The engine's nnz-balanced row ranges of a side (host row pointers):
+    world + 1 bounds, a row costing nnz * f^2 + f^3 / 3."""
+    ptr = np.ascontiguousarray(ptr, np.int64)
+    b = np.zeros(world + 1, np.int64)
+    _check(lib.als_shard_partition(_ptr(ptr), len(ptr) - 1, world, f, _ptr(b)))
+    return b
+
+
+def shard_blocks(bounds):
+    """(span, start): the all-gather's block size in rows and each rank's
+    first row of the block it sends."""
+    bounds = np.ascontiguousarray(bounds, np.int64)
+    world = len(bounds) - 1
+    span = c_i64()
+    start = np.zeros(world, np.int64)
+    _check(lib.als_shard_blocks(_ptr(bounds), world, ctypes.byref(span), _ptr(start)))
+    return int(span.value), start
+
+
+def shard_unique_id() -> bytes:
+    """A 128-byte NCCL unique id for Shard (made on rank 0, copied to all)."""
+    buf = ctypes.create_string_buffer(128)
+    _check(lib.als_shard_unique_id(buf))
+    return buf.raw
+
+
+class Shard:
+    """Row sharding of a Model across GPUs through the engine's C ABI (one
+    process per GPU): als_shard_create partitions both sides, restricts the
+    model to this rank's rows and creates the NCCL communicator; every call
+    below is collective."""
+
+    def __init__(self, model: "Model", ratings, world: int, rank: int, nccl_id: bytes):
+        self.model = model
+        csr = np.ascontiguousarray(ratings.csr_ptr, np.int64)
+        csc = np.ascontiguousarray(ratings.csc_ptr, np.int64)
+        idbuf = ctypes.create_string_buffer(bytes(nccl_id), 128)
+        h = c_vp()
+        _check(lib.als_shard_create(ctypes.byref(h), model.handle, _ptr(csr), _ptr(csc),
+                                    len(csr) - 1, len(csc) - 1, model.f, world, rank, idbuf,
+                                    model.stream))
+        self.handle, self.world, self.rank = h, world, rank
+
+    def bounds(self, side: int) -> np.ndarray:
+        b = np.zeros(self.world + 1, np.int64)
+        _check(lib.als_shard_bounds(self.handle, side, _ptr(b)))
+        return b
+
+    def exchange(self, side: int):
+        _check(lib.als_shard_exchange(self.handle, side, self.model.stream))
+
+    def half_step(self, side: int, lam: float):
+        _check(lib.als_shard_half_step(self.handle, side, lam, self.model.stream))
+
+    def iterate(self, lam: float, iters: int = 1):
+        _check(lib.als_shard_iterate(self.handle, lam, iters, self.model.stream))
+
+    def rmse(self, test=None) -> float:
+        u, i, r = test if test is not None else self.model.test
+        out = c_f64()
+        _check(lib.als_shard_rmse(self.handle, len(u), _ptr(u), _ptr(i), _ptr(r),
+                                  ctypes.byref(out), self.model.stream))
+        return float(out.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.als_shard_destroy(self.handle)
+            self.handle = None
 
 
 def _wrap_device(addr: int, shape, dtype):

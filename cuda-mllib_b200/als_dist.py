@@ -1,13 +1,15 @@
-"""Row sharding of the ALS half-step across GPUs (one process per GPU).
+"""Row sharding of the ALS half-step across ranks, restated over
+torch.distributed for the multi-rank tests.
 
-Every row's solve depends only on the fixed opposite factor, so a half-step
-shards by rows with no communication; the exchange step is after it: each
-rank's updated rows must reach every rank before the next half-step reads
-them as the fixed factor. Each rank keeps the full CSR/CSC and both factor
-matrices (Netflix shape: 1.6 GB + 200 MB per GPU), solves an nnz-balanced
-contiguous row range, then the ranges are exchanged by ONE all-gather per
-half-step (NCCL over NVLink/NVSwitch) and the low-precision copy is rebuilt
-from the FP32 rows.
+The engine's shard driver (als_shard_* in csrc/als_shard.cu, bound as
+als_b200.Shard; bench.py uses it under torchrun) is C++ over the C ABI with NCCL:
+every rank keeps the whole CSR/CSC and both factor matrices, solves an
+nnz-balanced contiguous row range of each side, and after each half-step the
+ranges are exchanged by ONE all-gather and the low-precision copy is rebuilt
+from the FP32 rows. NCCL needs one GPU per rank, so the exchange with several
+ranks is tested here instead: the same partition and blocks (checked equal to
+the engine's by tests/test_dist.py) and the same all-gather over gloo, with a
+CPU stand-in for the model.
 
 The ranges are nnz-balanced, so their row counts differ; the all-gather moves
 equal blocks of `span` = the largest range's row count. Each rank sends the
@@ -15,9 +17,6 @@ equal blocks of `span` = the largest range's row count. Each rank sends the
 back to stay inside the matrix for the last ranges), so the send needs no
 staging copy; after the collective each rank copies the other ranks' ranges
 out of the gathered blocks into place.
-
-The collective pattern is backend-independent (torch.distributed), so the same
-class runs over gloo on CPU in the tests with a CPU stand-in for the model.
 """
 from __future__ import annotations
 

@@ -135,6 +135,10 @@ cudaError_t run_rows(const Side &s, int f, float lambda, const als_options &o, c
 
 }  // namespace
 
+namespace als {
+int api_fail(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace als
+
 struct als_model {
   int64_t m = 0, n = 0, nnz = 0;
   int32_t f = 0;

@@ -144,7 +144,9 @@ rmse_partial_kernel(int64_t nt, const int32_t *u, const int32_t *i, const float 
   }
 }
 
-__global__ void rmse_final_kernel(const double *part, int nblocks, int64_t nt, double *out) {
+// out = sqrt(sum / nt), or the sum itself with `root` unset (a shard's share)
+__global__ void rmse_final_kernel(const double *part, int nblocks, int64_t nt, int root,
+                                  double *out) {
   __shared__ double red[256];
   double s = 0.0;
   for (int k = threadIdx.x; k < nblocks; k += blockDim.x) s += part[k];
@@ -154,7 +156,7 @@ __global__ void rmse_final_kernel(const double *part, int nblocks, int64_t nt, d
     if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[0] = nt > 0 ? sqrt(red[0] / (double)nt) : 0.0;
+  if (threadIdx.x == 0) out[0] = !root ? red[0] : nt > 0 ? sqrt(red[0] / (double)nt) : 0.0;
 }
 
 cudaError_t launch_rmse(int64_t nt, const int32_t *u, const int32_t *i, const float *r,
@@ -162,7 +164,16 @@ cudaError_t launch_rmse(int64_t nt, const int32_t *u, const int32_t *i, const fl
                         void *work, cudaStream_t st) {
   double *part = reinterpret_cast<double *>(work);
   rmse_partial_kernel<<<kRmseBlocks, kRmseThreads, 0, st>>>(nt, u, i, r, X, ldx, T, ldt, f, part);
-  rmse_final_kernel<<<1, 256, 0, st>>>(part, kRmseBlocks, nt, out_dev);
+  rmse_final_kernel<<<1, 256, 0, st>>>(part, kRmseBlocks, nt, 1, out_dev);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rmse_sum(int64_t nt, const int32_t *u, const int32_t *i, const float *r,
+                            const float *X, int ldx, const float *T, int ldt, int f,
+                            double *sum_dev, void *work, cudaStream_t st) {
+  double *part = reinterpret_cast<double *>(work);
+  rmse_partial_kernel<<<kRmseBlocks, kRmseThreads, 0, st>>>(nt, u, i, r, X, ldx, T, ldt, f, part);
+  rmse_final_kernel<<<1, 256, 0, st>>>(part, kRmseBlocks, nt, 0, sum_dev);
   return cudaGetLastError();
 }
 

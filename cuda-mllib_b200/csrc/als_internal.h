@@ -1,5 +1,6 @@
 // Internal launchers shared by the engine's translation units.
 #pragma once
+#include <string>
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -118,6 +119,14 @@ size_t rmse_work_bytes();
 cudaError_t launch_rmse(int64_t nt, const int32_t *u, const int32_t *i, const float *r,
                         const float *X, int ldx, const float *T, int ldt, int f, double *out_dev,
                         void *work, cudaStream_t st);
+// The sum of squared errors over the entries (no root, no division): a
+// shard's share of the test RMSE.
+cudaError_t launch_rmse_sum(int64_t nt, const int32_t *u, const int32_t *i, const float *r,
+                            const float *X, int ldx, const float *T, int ldt, int f,
+                            double *sum_dev, void *work, cudaStream_t st);
+// Sets the message als_last_error() returns and gives back the code (for the
+// C ABI entry points outside als_api.cu).
+int api_fail(int code, const std::string &msg);
 cudaError_t launch_predict(int64_t nt, const int32_t *u, const int32_t *i, const float *X, int ldx,
                            const float *T, int ldt, int f, float *out, cudaStream_t st);
 

@@ -188,6 +188,51 @@ int als_model_rmse(als_model *model, int64_t nt, const int32_t *d_u, const int32
 
 enum { ALS_ROW_EMPTY = 1, ALS_ROW_NOT_SPD = 2, ALS_ROW_REFINED_F64 = 4, ALS_ROW_CG_FALLBACK = 8 };
 
+/* Row sharding across GPUs, one process per GPU (no counterpart in the
+ * reference, which runs one problem on one GPU per call; the survey's
+ * multi-GPU design). Every rank holds the whole CSR/CSC and both factor
+ * matrices in its model, solves an nnz-balanced contiguous range of each
+ * side's rows, and after each half-step the ranges are exchanged by one NCCL
+ * all-gather (equal blocks of the largest range's row count; the other ranks'
+ * ranges are then copied into place) and the low-precision copy is rebuilt.
+ * Test RMSE: each rank's share of the entries, summed by an NCCL all-reduce.
+ * NCCL (libnccl.so.2) is loaded at the first call that needs it; without it
+ * these calls return ALS_ERR_UNSUPPORTED. Every rank makes the same calls in
+ * the same order (they are collective from als_shard_create on). */
+typedef struct als_shard als_shard;
+/* A 128-byte NCCL unique id: rank 0 makes it and sends a copy to every rank
+ * (through whatever channel the job has) before als_shard_create. */
+int als_shard_unique_id(void *id128);
+/* Host only: the nnz-balanced contiguous row ranges [b[r], b[r+1]) of a side
+ * with host row pointers h_ptr[rows + 1]; a row costs nnz * f^2 + f^3 / 3.
+ * h_bounds holds world + 1 values. */
+int als_shard_partition(const int64_t *h_ptr, int64_t rows, int32_t world, int32_t f,
+                        int64_t *h_bounds);
+/* Host only: the all-gather's block size in rows (the largest range) and, per
+ * rank, the first row of the block it sends: start[r] = min(b[r], rows - span). */
+int als_shard_blocks(const int64_t *h_bounds, int32_t world, int64_t *h_span, int64_t *h_start);
+/* Collective: partitions both sides from host copies of the model's row
+ * pointers (CSR m + 1 and CSC n + 1 values), restricts the model's half-steps
+ * to this rank's ranges, and creates the communicator. The model stays owned
+ * by the caller and must outlive the shard. */
+int als_shard_create(als_shard **out, als_model *model, const int64_t *h_csr_ptr,
+                     const int64_t *h_csc_ptr, int64_t m, int64_t n, int32_t f, int32_t world,
+                     int32_t rank, const void *id128, cudaStream_t stream);
+/* This rank's copy of a side's ranges (world + 1 values). */
+int als_shard_bounds(const als_shard *shard, int32_t side, int64_t *h_bounds);
+/* Collective: the all-gather of a side's ranges and the low-precision rebuild. */
+int als_shard_exchange(als_shard *shard, int32_t side, cudaStream_t stream);
+/* Collective: this rank's half-step of a side, then its exchange. */
+int als_shard_half_step(als_shard *shard, int32_t side, float lambda, cudaStream_t stream);
+/* Collective: `iters` full iterations (users, then items). */
+int als_shard_iterate(als_shard *shard, float lambda, int32_t iters, cudaStream_t stream);
+/* Collective: test RMSE over COO triplets (device arrays, the same on every
+ * rank); blocks until the value is on the host. */
+int als_shard_rmse(als_shard *shard, int64_t nt, const int32_t *d_u, const int32_t *d_i,
+                   const float *d_r, double *rmse_out, cudaStream_t stream);
+/* Collective (destroys the communicator). */
+void als_shard_destroy(als_shard *shard);
+
 /* Stand-alone half-step on caller buffers (no model): src n x f (ld_src),
  * dst m x f (ld_dst). work must hold als_half_step_work_bytes(m) bytes. */
 size_t als_half_step_work_bytes(int64_t m);

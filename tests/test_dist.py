@@ -43,6 +43,24 @@ def test_gather_blocks_cover_every_range():
             assert 0 <= start[r] <= b[r] and b[r + 1] <= start[r] + span <= rows
 
 
+def test_engine_partition_and_blocks_match():
+    """The C++ shard driver's partition and all-gather blocks
+    (als_shard_partition, als_shard_blocks; host code, no GPU) equal the
+    Python ones the gloo test drives, including empty and single-row ranges."""
+    r = A.synth(A.scaled_config("netflix", 0.05), seed=2)
+    rng = np.random.default_rng(8)
+    cases = [r.csr_ptr, r.csc_ptr, np.array([0, 0, 0, 5]), np.array([0, 7]),
+             np.concatenate([[0], np.cumsum(rng.integers(0, 50, 300))])]
+    for ptr in cases:
+        for world in (1, 2, 3, 5, 8):
+            for f in (10, 100, 128):
+                b = A.shard_partition(ptr, world, f)
+                assert np.array_equal(b, D.partition(ptr, world, f)), (world, f)
+                span, start = A.shard_blocks(b)
+                span_p, start_p = D.gather_blocks(b)
+                assert span == span_p and np.array_equal(start, start_p)
+
+
 class CpuModel:
     """CPU stand-in with the engine model's interface (FP64 oracle solves)."""
 
