@@ -98,6 +98,7 @@ struct als_shard {
   float *stage[2] = {nullptr, nullptr};  // world * span rows of f floats per side
   double *sums = nullptr;                // the RMSE partial sum (device)
   void *rmse_work = nullptr;             // the RMSE kernels' block sums (device)
+  bool ranged[2] = {false, false};       // the model's row range of a side was set
 };
 
 extern "C" {
@@ -179,6 +180,7 @@ int als_shard_create(als_shard **out, als_model *model, const int64_t *h_csr_ptr
     rc = als_model_set_row_range(model, side, s->bounds[side][rank], s->bounds[side][rank + 1],
                                  stream);
     if (rc != ALS_OK) return undo(rc);
+    s->ranged[side] = true;
   }
   cudaError_t e = cudaMalloc(&s->sums, sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&s->rmse_work, als_rmse_work_bytes());
@@ -267,6 +269,9 @@ int als_shard_rmse(als_shard *s, int64_t nt, const int32_t *d_u, const int32_t *
 void als_shard_destroy(als_shard *s) {
   if (!s) return;
   if (s->comm) nccl().comm_destroy(s->comm);
+  // the model solves all its rows again
+  for (int side = 0; side < 2; ++side)
+    if (s->ranged[side]) als_model_set_row_range(s->model, side, 0, s->rows[side], nullptr);
   for (float *p : s->stage)
     if (p) cudaFree(p);
   if (s->sums) cudaFree(s->sums);

@@ -1664,8 +1664,9 @@ cudaError_t launch_rows_tc_ws(const RowsArgs &a, int lp_kind, const TcSolve &sv,
 //                      bin) and the item total;
 //   plan_place_kernel  each item's rank (its bin's next free rank: a block
 //                      reserves its bin counts in one atomic per bin, then
-//                      ranks its rows in shared memory) and its place: rank k
-//                      goes to CTA k mod G, and within the CTA the order zigzags
+//                      ranks its rows in shared memory) and its place: ranks
+//                      are dealt to the CTAs in rounds of alternating
+//                      direction, and within the CTA the order zigzags
 //                      between its largest and smallest items, so rows that load
 //                      the producers (many ratings) alternate with rows that
 //                      load the solvers (few ratings).
@@ -1792,12 +1793,17 @@ __global__ void __launch_bounds__(1024) plan_scan_kernel(PlanDev p) {
   }
 }
 
-// Rank k (largest first) goes to CTA c = k mod G as that CTA's q-th largest
-// of its nc items; within the CTA the order zigzags between its largest and
-// smallest items (slots 0, 2, 4, ... take the largest, 1, 3, 5, ... the
-// smallest).
+// Rank k (largest first) goes to round q = k / G of the deal, and is its
+// CTA's q-th largest of nc items. Rounds run across the CTAs in alternating
+// directions (a snake), so no CTA takes the largest item of every round; the
+// last round, when partial, runs forward, so that CTA c still holds
+// ceil((N - c) / G) items (the kernel reads CTA c's items at c, c + G, ...
+// below N). Within the CTA the order zigzags between its largest and smallest
+// items (slots 0, 2, 4, ... take the largest, 1, 3, 5, ... the smallest).
 __device__ __forceinline__ void plan_put(const PlanDev &p, int64_t k, int64_t N, const WorkItem &w) {
-  const int64_t G = p.grid, c = k % G, q = k / G, nc = (N - c + G - 1) / G;
+  const int64_t G = p.grid, q = k / G;
+  const bool partial = N % G != 0 && q == N / G;
+  const int64_t c = ((q & 1) && !partial) ? G - 1 - k % G : k % G, nc = (N - c + G - 1) / G;
   const int64_t j = q < (nc + 1) / 2 ? 2 * q : 2 * (nc - 1 - q) + 1;  // zigzag slot
   p.items[c + j * G] = w;
 }

@@ -230,7 +230,8 @@ int als_shard_iterate(als_shard *shard, float lambda, int32_t iters, cudaStream_
  * rank); blocks until the value is on the host. */
 int als_shard_rmse(als_shard *shard, int64_t nt, const int32_t *d_u, const int32_t *d_i,
                    const float *d_r, double *rmse_out, cudaStream_t stream);
-/* Collective (destroys the communicator). */
+/* Collective: destroys the communicator and gives the model back its full row
+ * ranges (so the model must still exist). */
 void als_shard_destroy(als_shard *shard);
 
 /* Stand-alone half-step on caller buffers (no model): src n x f (ld_src),
