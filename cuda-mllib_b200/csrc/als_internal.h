@@ -19,6 +19,11 @@ cudaError_t launch_rows_fp32(const RowsArgs &a, int lp_kind, int num_sms, cudaSt
 // outside its range; the caller reports that instead of silently falling back.
 bool tc_supported(int f);
 int tc_padded_ld(int f);  // row stride (elements) of the low-precision factor copy
+// Rows longer than max(8192, nnz / (kPlanSplitDiv * CTAs)) ratings are split
+// into chunks of that size, so no item exceeds 1 / kPlanSplitDiv of a CTA's
+// share; fewer than kPlanSplitDiv * CTAs rows are split, into fewer than
+// 2 * kPlanSplitDiv * CTAs chunks.
+constexpr int kPlanSplitDiv = 4;
 struct WsPlan;
 // x0: CG starting points (rows of stride a.ld_dst), or null; scale_x0: scale
 // each start optimally along itself before CG (for a learned start).

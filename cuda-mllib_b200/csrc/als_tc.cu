@@ -465,7 +465,7 @@ cudaError_t launch_rows_tc(const RowsArgs &a, int lp_kind, int solver, int cg_ma
     // resets its row's counter, but a launch that gave up a bounded wait may
     // have left some part-way.
     if (plan->heavy_count && plan->ctas > 0) {
-      cudaError_t e = cudaMemsetAsync(plan->heavy_count, 0, sizeof(unsigned) * (4 * (size_t)plan->ctas + 1), st);
+      cudaError_t e = cudaMemsetAsync(plan->heavy_count, 0, sizeof(unsigned) * ((size_t)kPlanSplitDiv * plan->ctas + 1), st);
       if (e != cudaSuccess) return e;
     }
     sv.withhold_first = debug_take_withhold() ? 1 : 0;

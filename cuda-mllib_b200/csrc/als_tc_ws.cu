@@ -1697,7 +1697,7 @@ struct PlanDev {
 
 __device__ __forceinline__ int64_t plan_split(const PlanDev &p) {
   const int64_t nnz = p.ptr[p.begin + p.count] - p.ptr[p.begin];
-  const int64_t q = 4LL * p.grid;
+  const int64_t q = (int64_t)kPlanSplitDiv * p.grid;
   const int64_t s = (nnz + q - 1) / q;
   return s > 8192 ? s : 8192;
 }
@@ -1863,10 +1863,12 @@ struct PlanLayout {
   PlanLayout(int64_t count, int grid, int np) {
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     // A row of d > split ratings becomes ceil(d / split) < d / split + 1
-    // chunks, and split >= nnz / (4 grid): fewer than 4 grid split rows,
-    // fewer than 8 grid chunks of them, fewer than count + 4 grid items.
-    const size_t hmax = 4 * (size_t)grid + 1, smax = 8 * (size_t)grid,
-                 imax = (size_t)count + 4 * (size_t)grid;
+    // chunks, and split >= nnz / (D grid), D = kPlanSplitDiv: fewer than
+    // D grid split rows, fewer than 2 D grid chunks of them, fewer than
+    // count + D grid items.
+    const size_t D = kPlanSplitDiv;
+    const size_t hmax = D * (size_t)grid + 1, smax = 2 * D * (size_t)grid,
+                 imax = (size_t)count + D * (size_t)grid;
     size_t o = 0;
     oHdr = o; o += al(sizeof(PlanHdr));
     oHist = o; o += al(4 * kPlanBins);
@@ -1913,9 +1915,9 @@ cudaError_t plan_ws(const int64_t *d_row_ptr, int64_t begin, int64_t count, int 
   p.begin = begin;
   p.count = count;
   p.grid = grid;
-  p.hmax = 4 * grid + 1;
-  p.smax = 8 * grid;
-  p.imax = count + 4LL * grid;
+  p.hmax = kPlanSplitDiv * grid + 1;
+  p.smax = 2 * kPlanSplitDiv * grid;
+  p.imax = count + (int64_t)kPlanSplitDiv * grid;
   p.error = error;
   p.hdr = reinterpret_cast<PlanHdr *>(d + L.oHdr);
   p.hist = reinterpret_cast<unsigned *>(d + L.oHist);
