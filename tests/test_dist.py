@@ -61,6 +61,27 @@ def test_engine_partition_and_blocks_match():
                 assert span == span_p and np.array_equal(start, start_p)
 
 
+def test_engine_shard_rejects_bad_arguments():
+    """The shard entry points check their arguments before touching a GPU or
+    NCCL: null pointers, world < 1 and a rank outside [0, world) are
+    ALS_ERR_INVALID with a message."""
+    import ctypes
+    lib = A.lib
+    ptr = np.array([0, 3, 5], np.int64)
+    b = np.zeros(3, np.int64)
+    assert lib.als_shard_partition(None, 2, 2, 10, b.ctypes.data) == 1
+    assert lib.als_shard_partition(ptr.ctypes.data, 2, 0, 10, b.ctypes.data) == 1
+    assert b"bad arguments" in lib.als_last_error()
+    h = ctypes.c_void_p()
+    idbuf = ctypes.create_string_buffer(128)
+    for world, rank in ((0, 0), (2, 2), (2, -1)):
+        rc = lib.als_shard_create(ctypes.byref(h), ctypes.c_void_p(1), ptr.ctypes.data, ptr.ctypes.data,
+                                  2, 2, 10, world, rank, idbuf, None)
+        assert rc == 1 and not h.value, (world, rank)
+    span = ctypes.c_int64()
+    assert lib.als_shard_blocks(None, 2, ctypes.byref(span), b.ctypes.data) == 1
+
+
 class CpuModel:
     """CPU stand-in with the engine model's interface (FP64 oracle solves)."""
 
