@@ -254,11 +254,11 @@ def run_reference(args):
 # Per-launch DRAM traffic of the rows kernel at the default workload (the
 # Netflix shape, BF16 CG, previous iterate), from one ncu capture of the same
 # command at full size (dram__bytes_read.sum + dram__bytes_write.sum, one pass;
-# profiles/rows_tc_ws_netflix_dram.txt): the mean of the users launch (1.466 GB)
-# and the items launch (3.511 GB). None for other workloads.
-DRAM_PER_LAUNCH = 2.489e9
+# profiles/rows_tc_ws_netflix_dram.txt): the mean of the users launch (1.468 GB)
+# and the items launch (3.349 GB). None for other workloads.
+DRAM_PER_LAUNCH = 2.408e9
 DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, full-size workload, 4th iteration: "
-               "users 1.466e9, items 3.511e9 bytes")
+               "users 1.468e9, items 3.349e9 bytes")
 
 FIXTURE = os.path.join(ROOT, "tests", "golden", "netflix_f100_fp64.npz")
 RESTART = 10  # iterations of one training run (the workload's iteration count)
