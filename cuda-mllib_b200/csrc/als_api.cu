@@ -180,6 +180,14 @@ int tune_groups(int f, int k) {
 }
 }  // namespace
 
+namespace als {
+void model_dims(const als_model *M, int64_t *m, int64_t *n, int32_t *f) {
+  *m = M->m;
+  *n = M->n;
+  *f = M->f;
+}
+}  // namespace als
+
 extern "C" {
 
 void als_default_options(als_options *o) {

@@ -132,6 +132,11 @@ cudaError_t launch_rmse_sum(int64_t nt, const int32_t *u, const int32_t *i, cons
 // Sets the message als_last_error() returns and gives back the code (for the
 // C ABI entry points outside als_api.cu).
 int api_fail(int code, const std::string &msg);
+}  // namespace als
+struct als_model;
+namespace als {
+// A model's rows of each side and its rank (for the shard driver's checks).
+void model_dims(const als_model *model, int64_t *m, int64_t *n, int32_t *f);
 cudaError_t launch_predict(int64_t nt, const int32_t *u, const int32_t *i, const float *X, int ldx,
                            const float *T, int ldt, int f, float *out, cudaStream_t st);
 

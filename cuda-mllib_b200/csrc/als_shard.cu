@@ -153,6 +153,13 @@ int als_shard_create(als_shard **out, als_model *model, const int64_t *h_csr_ptr
       rank < 0 || rank >= world || !id128)
     return api_fail(ALS_ERR_INVALID, "als_shard_create: bad arguments");
   *out = nullptr;
+  {
+    int64_t mm = 0, nn = 0;
+    int32_t ff = 0;
+    model_dims(model, &mm, &nn, &ff);
+    if (mm != m || nn != n || ff != f)
+      return api_fail(ALS_ERR_INVALID, "als_shard_create: m, n, f differ from the model's");
+  }
   if (!nccl().ok) return api_fail(ALS_ERR_UNSUPPORTED, "als_shard_create: libnccl.so.2 not found");
   auto *s = new als_shard();
   s->model = model;

@@ -41,3 +41,20 @@ def test_one_rank_shard_equals_unsharded(prec):
     assert st["kernel_errors"] == 0
     assert np.array_equal(X, Xr) and np.array_equal(T, Tr)
     assert abs(rm - rm_ref) <= 1e-12 * max(1.0, rm_ref), (rm, rm_ref)
+
+
+def test_shard_rejects_dimensions_other_than_the_models():
+    """m, n or f that differ from the model's are ALS_ERR_INVALID before any
+    communicator is made."""
+    import ctypes
+    r = A.synth(A.scaled_config("ml1m", 0.05), seed=3)
+    M = A.Model(r, 16, A.options(precision=A.PREC_BF16, solver=A.SOLVER_CG), theta0=A.init_factors(r.n, 16, 1))
+    csr = np.ascontiguousarray(r.csr_ptr, np.int64)
+    csc = np.ascontiguousarray(r.csc_ptr, np.int64)
+    idbuf = ctypes.create_string_buffer(A.shard_unique_id(), 128)
+    h = ctypes.c_void_p()
+    for m, n, f in ((r.m + 1, r.n, 16), (r.m, r.n - 1, 16), (r.m, r.n, 32)):
+        rc = A.lib.als_shard_create(ctypes.byref(h), M.handle, csr.ctypes.data, csc.ctypes.data,
+                                    m, n, f, 1, 0, idbuf, M.stream)
+        assert rc == 1 and not h.value and b"differ" in A.lib.als_last_error()
+    M.close()
