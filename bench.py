@@ -8,8 +8,9 @@ the resident matrix. GFLOP/s uses the solver-independent formula
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
 Engine arm: inputs resident in HBM, CUDA events on the model's stream, max
-over ranks; e2e through the drop-in doALSWithCSR with host buffers (CSR upload
-as the Spark JNI does it, theta upload, X download inside the timed region).
+over ranks; e2e through the Spark JNI entry's host-buffer half-step
+(als_half_step_host: CSR upload, theta upload and X download inside the timed
+region, the uploads overlapped range by range with the solve).
 Reference arm: the reference has no CPU ALS (its CPU path is Spark's JVM ALS,
 absent here), so it times the CPU port of the same half-step (oracle FP32) on
 bounded seeded row samples with all host threads, scaled by the formula.
@@ -508,15 +509,19 @@ def run_engine(args):
                     forms[k2]["speedup_vs_fp32_cholesky"] = round(base / forms[k2]["sec_per_iter"], 2)
         line["forms"] = forms
 
-    # e2e through the drop-in entry point with host buffers (rank 0, 1 GPU path),
-    # in the same precision and solver (the drop-in call has no previous X: CG
-    # starts from zero there). Theta and X live in pinned host memory, as the
-    # reference's JNI caller allocates them (cudaMallocHost,
-    # CuMFJNIInterface.cpp:53-57); the CSR arrays are uploaded from pinned
-    # memory into mallocBest memory, which the call frees.
+    # e2e through the reference-facing host-buffer path: the half-step the
+    # Spark JNI entry runs (als_half_step_host: the CSR arrays uploaded in row
+    # ranges, each range solved while the next one crosses PCIe, X downloaded
+    # range by range), rank 0 on the 1-GPU path, in the same precision and
+    # solver (the drop-in call has no previous X: CG starts from zero there).
+    # Theta and X live in pinned host memory, as the reference's JNI caller
+    # allocates them (cudaMallocHost, CuMFJNIInterface.cpp:53-57), and so do
+    # the CSR arrays.
     if rank == 0 and not args.no_e2e:
+        sg = model.stats()["solver_groups"]
         A.set_dropin_options(A.options(precision=prec, solver=solver, warm_start=A.WARM_ZERO,
-                                       cg_jacobi=1 if args.jacobi else 0))
+                                       cg_jacobi=1 if args.jacobi else 0,
+                                       solver_groups=int(sg[0]) if sg[0] == sg[1] else 0))
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
         T = pin(model.factors()[1].cpu().numpy())
         Xh = pin(np.zeros((r.m, f), np.float32))
@@ -530,8 +535,8 @@ def run_engine(args):
         src_t = T
         for _ in range(e2e_steps + 1):
             t1 = time.perf_counter()
-            A.do_als_with_csr(host[0], host[1], host[2], src_t, r.m, r.n, f, lam, out=Xh)
-            A.do_als_with_csr(host[3], host[4], host[5], Xh, r.n, r.m, f, lam, out=Th)
+            A.half_step_host(host[0], host[1], host[2], src_t, r.m, r.n, f, lam, out=Xh)
+            A.half_step_host(host[3], host[4], host[5], Xh, r.n, r.m, f, lam, out=Th)
             times.append(time.perf_counter() - t1)
             src_t = Th
         e2e_s = float(np.median(times[1:]))
@@ -540,9 +545,11 @@ def run_engine(args):
         line["e2e"] = {"value": round(flop_iter / e2e_s / 1e9, 2), "unit": "GFLOP/s",
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "sec_per_iter": round(e2e_s, 4),
-                       "path": "doALSWithCSR x2 (users, items): CSR upload from pinned memory to "
-                               "mallocBest memory, theta upload and X download from/to pinned "
-                               "buffers; wall clock; same form (CG from zero)"}
+                       "path": "als_half_step_host x2 (users, items), the Spark JNI entry's "
+                               "half-step: CSR, theta and X in pinned host memory, the ratings "
+                               "uploaded in row ranges overlapped with the solve of the previous "
+                               "range, X downloaded range by range; wall clock; same form (CG "
+                               "from zero)"}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         users, items, Xs, Ts, frac = cpu_sample_plan(r, f, lam, args.cpu_seconds, args.seed)

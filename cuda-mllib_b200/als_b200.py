@@ -114,6 +114,8 @@ _sig(lib.als_train, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i
      c_i32, c_vp, c_vp, c_vp, c_vp)
 _sig(lib.doALSWithCSR, None, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int,
      ctypes.c_int, ctypes.c_long, c_f32, ctypes.c_int)
+_sig(lib.als_half_step_host, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int,
+     ctypes.c_int, ctypes.c_int, ctypes.c_long, c_f32, ctypes.c_int)
 _sig(lib.als_set_dropin_options, c_i32, c_vp)
 _sig(lib.als_debug_withhold_first_row, c_i32, c_i32)
 _sig(lib.als_get_dropin_options, c_i32, c_vp)
@@ -574,4 +576,27 @@ def do_als_with_csr(row_ptr32: np.ndarray, col: np.ndarray, val: np.ndarray, the
             raise ValueError("out must be a C-contiguous float32 array of shape (m, f)")
         X = out
     lib.doALSWithCSR(None, ptrs[0], ptrs[1], ptrs[2], _ptr(th), _ptr(X), m, n, f, nnz, lam, x_batch)
+    return X
+
+
+def half_step_host(row_ptr32: np.ndarray, col: np.ndarray, val: np.ndarray, theta: np.ndarray,
+                   m: int, n: int, f: int, lam: float, out: np.ndarray | None = None,
+                   chunks: int = 0) -> np.ndarray:
+    """The drop-in half-step on host CSR arrays (``als_half_step_host``, the
+    path of the Spark JNI call): the ratings are uploaded in ``chunks`` row
+    ranges (0: chosen from the rating count), each solved while the next one
+    is uploaded. Same options and result as ``do_als_with_csr``; the arrays
+    stay the caller's. Returns X (m x f), written into ``out`` when given."""
+    ptr = np.ascontiguousarray(row_ptr32, np.int32)
+    c = np.ascontiguousarray(col, np.int32)
+    v = np.ascontiguousarray(val, np.float32)
+    th = np.ascontiguousarray(theta, np.float32)
+    if out is None:
+        X = np.zeros((m, f), np.float32)
+    else:
+        if out.dtype != np.float32 or out.shape != (m, f) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of shape (m, f)")
+        X = out
+    _check(lib.als_half_step_host(None, _ptr(ptr), _ptr(c), _ptr(v), _ptr(th), _ptr(X), m, n, f,
+                                  len(c), lam, chunks))
     return X

@@ -1167,6 +1167,185 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
 }
 
 // ---------------------------------------------------------------------------
+// als_half_step_host: the drop-in half-step on HOST CSR arrays, i.e. the whole
+// path of the Spark JNI call, which uploads the three arrays into mallocBest
+// memory (CuMFJNIInterface.cpp:93-118) before doALSWithCSR uploads theta,
+// solves and downloads X, each transfer waiting for the one before. Here the
+// ratings cross PCIe in row ranges of about equal rating counts on a copy
+// stream; each range is planned and solved on the caller's stream as soon as
+// it has landed, and its rows of X go back on a third stream while the next
+// range is solved. At the Netflix shape a side's ratings (0.8 GB) take about
+// as long to upload as the users side takes to solve, so the half-step costs
+// about the longer of the two instead of their sum.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kHostChunksMax = 16;
+constexpr long kHostChunkRatings = 12500000;  // automatic ranges: about this many ratings each
+
+// The streams, events and workspace of one call. The destructor waits for all
+// three streams before the workspace goes back to the cache, on every path.
+struct HostPipe {
+  cudaStream_t st, up = nullptr, dn = nullptr;
+  std::vector<cudaEvent_t> ev;
+  char *d = nullptr;
+  explicit HostPipe(cudaStream_t s) : st(s) {}
+  cudaError_t init(int events) {
+    cudaError_t e = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&dn, cudaStreamNonBlocking);
+    for (int i = 0; i < events && e == cudaSuccess; ++i) {
+      cudaEvent_t x = nullptr;
+      e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+      if (e == cudaSuccess) ev.push_back(x);
+    }
+    return e;
+  }
+  HostPipe(const HostPipe &) = delete;
+  HostPipe &operator=(const HostPipe &) = delete;
+  ~HostPipe() {
+    if (up) cudaStreamSynchronize(up);
+    cudaStreamSynchronize(st);
+    if (dn) cudaStreamSynchronize(dn);
+    if (d) block_release(d, false);
+    for (cudaEvent_t x : ev) cudaEventDestroy(x);
+    if (up) cudaStreamDestroy(up);
+    if (dn) cudaStreamDestroy(dn);
+  }
+};
+
+// Row ranges [b[c], b[c + 1]) of about nnz / chunks ratings each (empty ranges
+// dropped); the row pointers are non-decreasing and end at nnz.
+std::vector<int> host_ranges(const int *row_ptr, int m, long nnz, int chunks) {
+  std::vector<int> b{0};
+  for (int c = 1; c < chunks; ++c) {
+    const int target = (int)(nnz * c / chunks);
+    const int r = (int)(std::lower_bound(row_ptr, row_ptr + m + 1, target) - row_ptr);
+    if (r > b.back() && r < m) b.push_back(r);
+  }
+  b.push_back(m);
+  return b;
+}
+}  // namespace
+
+extern "C" int als_half_step_host(cudaStream_t st, const int *h_row_ptr, const int *h_col,
+                                  const float *h_val, const float *thetaTHost, float *XTHost,
+                                  int m, int n, int f, long nnz, float lambda, int chunks) {
+  if (!h_row_ptr || !thetaTHost || m < 0 || n <= 0 || f <= 0 || nnz < 0 || nnz > INT32_MAX ||
+      (m > 0 && !XTHost) || (nnz > 0 && (!h_col || !h_val)) || chunks < 0 ||
+      chunks > kHostChunksMax)
+    return fail(ALS_ERR_INVALID, "als_half_step_host: bad arguments");
+  if (h_row_ptr[0] != 0 || (long)h_row_ptr[m] != nnz)
+    return fail(ALS_ERR_INVALID, "als_half_step_host: the row pointers do not span nnz ratings");
+  for (int i = 0; i < m; ++i)
+    if (h_row_ptr[i + 1] < h_row_ptr[i])
+      return fail(ALS_ERR_INVALID, "als_half_step_host: decreasing row pointer");
+  als_options o;
+  als_get_dropin_options(&o);
+  if (o.warm_start == ALS_WARM_PREVIOUS) o.warm_start = ALS_WARM_ZERO;  // no previous X here
+  if (int rc = check_options(o, f); rc != ALS_OK) return rc;
+  if (m == 0) return ALS_OK;
+  const int K = chunks ? chunks
+                       : (int)std::min<long>(kHostChunksMax / 2,
+                                             std::max<long>(1, (nnz + kHostChunkRatings - 1) /
+                                                                   kHostChunkRatings));
+  const std::vector<int> rb = host_ranges(h_row_ptr, m, nnz, K);
+  const int nch = (int)rb.size() - 1;
+  const int kind = lp_kind_of(o.precision);
+  const int ldp = kind ? tc_padded_ld(f) : 0;
+  const int sms = device_sm_count();
+  const bool ws = kind != kLpNone && tc_ws_takes(f, o.solver, o.cg_jacobi);
+  const int np = ws ? tc_ws_np(f) : 0;
+  // the drop-in's workspace, then the CSR arrays
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t p = off; off = align_up(off + bytes, 256); return p; };
+  const size_t oT = take(sizeof(float) * (size_t)n * f), oX = take(sizeof(float) * (size_t)m * f + 4),
+               oP = take(sizeof(int64_t) * ((size_t)m + 1)), oW = take(als_half_step_work_bytes(m)),
+               oL = take(kind ? 2ull * n * ldp : 0), oPl = take(ws ? plan_ws_bytes(m, sms, np) : 0),
+               oR = take(sizeof(int) * ((size_t)m + 1)),
+               oC = take(sizeof(int) * (size_t)std::max<long>(nnz, 1)),
+               oV = take(sizeof(float) * (size_t)std::max<long>(nnz, 1));
+  HostPipe p(st);
+  ALS_TRY(p.init(1 + 2 * nch), "als_half_step_host: streams");
+  void *blk = nullptr;
+  ALS_TRY(block_alloc(&blk, off), "als_half_step_host: workspace");
+  p.d = static_cast<char *>(blk);
+  char *d = p.d;
+  int *d_row = reinterpret_cast<int *>(d + oR), *d_col = reinterpret_cast<int *>(d + oC);
+  float *d_val = reinterpret_cast<float *>(d + oV), *d_x = reinterpret_cast<float *>(d + oX);
+  // row pointers and theta first: every range needs them
+  ALS_TRY(cudaMemcpyAsync(d_row, h_row_ptr, sizeof(int) * ((size_t)m + 1), cudaMemcpyHostToDevice, p.up),
+          "als_half_step_host: row pointers");
+  ALS_TRY(staged_copy(d + oT, thetaTHost, sizeof(float) * (size_t)n * f, true, p.up),
+          "als_half_step_host: theta upload");
+  ALS_TRY(cudaEventRecord(p.ev[0], p.up), "als_half_step_host: event");
+  ALS_TRY(cudaStreamWaitEvent(st, p.ev[0], 0), "als_half_step_host: event");
+  ALS_TRY(launch_widen_ptr(d_row, (int64_t)m + 1, reinterpret_cast<int64_t *>(d + oP), st),
+          "als_half_step_host: row pointers");
+  if (kind != kLpNone)
+    ALS_TRY(launch_convert_lp(reinterpret_cast<const float *>(d + oT), n, f, f, d + oL, ldp, kind, st),
+            "als_half_step_host: theta copy");
+  Side S;
+  S.rows = m; S.cols = n; S.ptr = reinterpret_cast<const int64_t *>(d + oP);
+  S.idx = d_col; S.val = d_val;
+  char *w = d + oW;
+  S.order = reinterpret_cast<int32_t *>(w);
+  S.queue = reinterpret_cast<unsigned *>(w + align_up(sizeof(int32_t) * m, 256));
+  Counters *ctr = reinterpret_cast<Counters *>(reinterpret_cast<char *>(S.queue) +
+                                               align_up(sizeof(unsigned) * (1 + 3 * kOrderBins), 256));
+  ALS_TRY(cudaMemsetAsync(ctr, 0, sizeof(Counters), st), "als_half_step_host: counters");
+  // X goes back range by range when the caller's buffer is pinned; a pageable
+  // one is written at the end through the pinned staging (a copy into
+  // pageable memory holds the host thread until it is done, which would keep
+  // the next range's upload from being issued)
+  const bool x_pinned = !pageable(XTHost);
+  for (int c = 0; c < nch; ++c) {
+    const int r0 = rb[c], r1 = rb[c + 1];
+    const size_t k0 = (size_t)h_row_ptr[r0], kn = (size_t)h_row_ptr[r1] - k0;
+    if (kn) {
+      ALS_TRY(staged_copy(d_col + k0, h_col + k0, sizeof(int) * kn, true, p.up),
+              "als_half_step_host: ratings upload");
+      ALS_TRY(staged_copy(d_val + k0, h_val + k0, sizeof(float) * kn, true, p.up),
+              "als_half_step_host: ratings upload");
+    }
+    ALS_TRY(cudaEventRecord(p.ev[1 + 2 * c], p.up), "als_half_step_host: event");
+    ALS_TRY(cudaStreamWaitEvent(st, p.ev[1 + 2 * c], 0), "als_half_step_host: event");
+    S.begin = r0;
+    S.active = r1 - r0;
+    ALS_TRY(launch_degree_order(S.ptr, S.active, S.order, S.queue + 1, st, r0),
+            "als_half_step_host: order");
+    if (ws) {
+      ALS_TRY(plan_ws(S.ptr, r0, S.active, sms, np, n, d + oPl, plan_ws_bytes(m, sms, np), &S.plan,
+                      &ctr->error, st),
+              "als_half_step_host: plan");
+      S.has_plan = true;
+    }
+    ALS_TRY(run_rows(S, f, lambda, o, reinterpret_cast<const float *>(d + oT), f, d + oL, ldp, d_x,
+                     nullptr, ctr, nullptr, false, sms, st),
+            "als_half_step_host: half-step");
+    if (x_pinned) {
+      ALS_TRY(cudaEventRecord(p.ev[2 + 2 * c], st), "als_half_step_host: event");
+      ALS_TRY(cudaStreamWaitEvent(p.dn, p.ev[2 + 2 * c], 0), "als_half_step_host: event");
+      ALS_TRY(cudaMemcpyAsync(XTHost + (size_t)r0 * f, d_x + (size_t)r0 * f,
+                              sizeof(float) * (size_t)(r1 - r0) * f, cudaMemcpyDeviceToHost, p.dn),
+              "als_half_step_host: X download");
+    }
+  }
+  int kernel_error = 0;
+  ALS_TRY(cudaMemcpyAsync(&kernel_error, &ctr->error, sizeof(int), cudaMemcpyDeviceToHost, st),
+          "als_half_step_host: error word");
+  if (!x_pinned)
+    ALS_TRY(staged_copy(XTHost, d_x, sizeof(float) * (size_t)m * f, false, st),
+            "als_half_step_host: X download");
+  ALS_TRY(cudaStreamSynchronize(st), "als_half_step_host: sync");
+  ALS_TRY(cudaStreamSynchronize(p.dn), "als_half_step_host: sync");
+  if (kernel_error)
+    return fail(ALS_ERR_CUDA, (kernel_error & 1)
+                                  ? "als_half_step_host: a kernel gave up a bounded wait (bounded "
+                                    "wait timed out); the half-step's rows are incomplete"
+                                  : "als_half_step_host: malformed CSR row pointers");
+  return ALS_OK;
+}
+
+// ---------------------------------------------------------------------------
 // als_half_step_static: the stand-alone FP32 half-step with its scratch (the
 // degree-binned visiting order, the row-queue head and the counters) in a
 // file-scope device array, so that a call allocates nothing. It serves callers

@@ -1,11 +1,15 @@
-// Spark JNI entry of libGPUALS.so: marshals Spark's factor blocks and CSR
-// arrays into native memory, runs the drop-in doALSWithCSR half-step, and
-// returns float[m][f]. Behaviour follows als/src/CuMFJNIInterface.cpp:25-132:
-// device chosen round-robin per call, source factors flattened in block
-// order, CSR uploaded to mallocBest memory that the half-step frees, the
-// result returned as one float[f] per row.
+// Spark JNI entry of libGPUALS.so: marshals Spark's factor blocks into
+// native memory, runs the drop-in half-step on the CSR arrays, and returns
+// float[m][f]. Behaviour follows als/src/CuMFJNIInterface.cpp:25-132: device
+// chosen round-robin per call, source factors flattened in block order, the
+// half-step of doALSWithCSR (same options and result), the result returned as
+// one float[f] per row.
 //
 // Per-call costs of the reference that this shim does not pay:
+//  - it uploads the whole CSR into mallocBest memory (:93-118) and only then
+//    starts the half-step, which uploads theta, solves and downloads X, one
+//    step after the other. Here als_half_step_host uploads the ratings in row
+//    ranges and solves each range while the next one crosses PCIe;
 //  - it pins fresh host buffers for theta and X on every call (cudaMallocHost,
 //    CuMFJNIInterface.cpp:53-57; page-locking 192 MB takes tens of ms) and
 //    creates and destroys a stream (:32-34). Here both are leased from
@@ -234,39 +238,23 @@ extern "C" jobjectArray Java_org_apache_spark_ml_recommendation_CuMFJNIInterface
     if (index != (size_t)n)
       throw thrust::system_error(cudaErrorInvalidValue, thrust::cuda_category(),
                                  "source factor count differs from n");
-    // The CSR arrays go to doALSWithCSR, which frees them; until then they
-    // are this call's, and a failure before the hand-over frees them here.
-    struct CsrArrays {
-      int *row = nullptr, *col = nullptr;
-      float *val = nullptr;
-      bool handed_over = false;
-      ~CsrArrays() {
-        if (handed_over) return;
-        freeBest(row);
-        freeBest(col);
-        freeBest(val);
-      }
-    } csr;
-    check(mallocBest((void **)&csr.row, sizeof(int) * ((size_t)m + 1)), "mallocBest row");
-    check(mallocBest((void **)&csr.col, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)), "mallocBest col");
-    check(mallocBest((void **)&csr.val, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1)), "mallocBest val");
+    // The CSR arrays go straight from the Java arrays to the pipelined
+    // half-step (ranges of ratings uploaded while the previous range is
+    // solved), which reads them and leaves them to the caller.
     void *hr = J.GetPrimitiveArrayCritical(csrRow, nullptr);
     void *hc = J.GetPrimitiveArrayCritical(csrCol, nullptr);
     void *hv = J.GetPrimitiveArrayCritical(csrVal, nullptr);
-    cudaError_t e = cudaMemcpyAsync(csr.row, hr, sizeof(int) * ((size_t)m + 1),
-                                    cudaMemcpyHostToDevice, stream.s);
-    if (e == cudaSuccess && nnz > 0)
-      e = cudaMemcpyAsync(csr.col, hc, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, stream.s);
-    if (e == cudaSuccess && nnz > 0)
-      e = cudaMemcpyAsync(csr.val, hv, sizeof(float) * (size_t)nnz, cudaMemcpyHostToDevice, stream.s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream.s);
-    J.ReleasePrimitiveArrayCritical(csrRow, hr, 0);
-    J.ReleasePrimitiveArrayCritical(csrCol, hc, 0);
-    J.ReleasePrimitiveArrayCritical(csrVal, hv, 0);
-    check(e, "CSR upload");
-    csr.handed_over = true;  // doALSWithCSR frees them, on success and on failure
-    doALSWithCSR(stream.s, csr.row, csr.col, csr.val, thetaTHost, XTHost, m, n, f, nnz,
-                 (float)lambda, 1);
+    int rc = ALS_ERR_INVALID;
+    if (hr && hc && hv)
+      rc = als_half_step_host(stream.s, static_cast<const int *>(hr), static_cast<const int *>(hc),
+                              static_cast<const float *>(hv), thetaTHost, XTHost, m, n, f, nnz,
+                              (float)lambda, 0);
+    if (hv) J.ReleasePrimitiveArrayCritical(csrVal, hv, 0);
+    if (hc) J.ReleasePrimitiveArrayCritical(csrCol, hc, 0);
+    if (hr) J.ReleasePrimitiveArrayCritical(csrRow, hr, 0);
+    if (rc != ALS_OK)
+      throw thrust::system_error(rc == ALS_ERR_INVALID ? cudaErrorInvalidValue : cudaErrorLaunchFailure,
+                                 thrust::cuda_category(), als_last_error());
     // float[m][f], a frame of rows at a time
     jclass floatArrayClass = J.FindClass("[F");
     jobjectArray output = J.NewObjectArray(m, floatArrayClass, nullptr);

@@ -139,6 +139,26 @@ void als_default_options(als_options *opt);
  * changing the call. No counterpart in the reference. */
 int als_set_dropin_options(const als_options *opt);
 int als_get_dropin_options(als_options *opt);
+
+/* The drop-in half-step on HOST CSR arrays: what the Spark JNI call does as a
+ * whole (CuMFJNIInterface.cpp:93-118 copies the three arrays into mallocBest
+ * memory, then calls doALSWithCSR, als.cu:1001-1115), with the same inputs,
+ * options (als_set_dropin_options) and result X, but pipelined: the ratings
+ * are uploaded in `chunks` row ranges of about equal rating counts (0: one
+ * per ~12.5M ratings, at most 8) on a copy stream, each range is solved on
+ * `stream` as soon as it has landed, and its rows of X are downloaded while
+ * the next range is solved. The arrays are the caller's and are not freed.
+ * Host memory may be pageable (copied through pinned staging) or pinned
+ * (copied directly; a pinned XTHost is also downloaded range by range).
+ * Rows split across CTAs (longer than max(8192, range ratings / (4 * SMs)))
+ * may differ from doALSWithCSR in the last bits, since the split depends on
+ * the range; all other rows are bit-identical. Returns ALS_OK,
+ * ALS_ERR_INVALID (bad sizes, row pointers that decrease or do not span nnz)
+ * or ALS_ERR_CUDA (also when a kernel gave up a bounded wait); no exception.
+ * Synchronises before it returns. The JNI entry of this library uses it. */
+int als_half_step_host(cudaStream_t stream, const int *h_row_ptr, const int *h_col,
+                       const float *h_val, const float *thetaTHost, float *XTHost, int m, int n,
+                       int f, long nnz, float lambda, int chunks);
 const char *als_last_error(void);
 const char *als_version(void);
 

@@ -6,6 +6,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 import als_b200 as A
@@ -122,6 +123,34 @@ def test_argument_errors_without_gpu():
     assert rc == A.ALS_ERR_UNSUPPORTED
     rc = A.lib.als_train(None, None, None, None, None, None, 1, 1, 1, 0, 0.1, 1, None, None, None, None)
     assert rc == A.ALS_ERR_INVALID
+
+
+def test_host_half_step_argument_errors_without_gpu():
+    """als_half_step_host checks sizes and the host row pointers before any
+    CUDA call: decreasing pointers, pointers that do not start at 0 or end at
+    nnz, and range counts above 16 are ALS_ERR_INVALID; m = 0 has nothing to
+    solve and returns ALS_OK."""
+    f, n = 4, 3
+    th = np.zeros((n, f), np.float32)
+    X = np.zeros((2, f), np.float32)
+    col = np.array([0, 1, 2], np.int32)
+    val = np.ones(3, np.float32)
+    fn = A.lib.als_half_step_host
+
+    def call(ptr, m=2, nnz=3, chunks=0, theta=th):
+        p = np.ascontiguousarray(ptr, np.int32)
+        return fn(None, p.ctypes.data, col.ctypes.data, val.ctypes.data,
+                  theta.ctypes.data if theta is not None else None, X.ctypes.data, m, n, f, nnz,
+                  0.05, chunks)
+
+    assert call([0, 2, 1]) == A.ALS_ERR_INVALID and b"span" in A.lib.als_last_error()
+    assert call([0, 2, 1, 3], m=3) == A.ALS_ERR_INVALID and b"decreasing" in A.lib.als_last_error()
+    assert call([1, 2, 3]) == A.ALS_ERR_INVALID
+    assert call([0, 1, 3], chunks=17) == A.ALS_ERR_INVALID
+    assert call([0, 1, 3], chunks=-1) == A.ALS_ERR_INVALID
+    assert call([0, 1, 3], theta=None) == A.ALS_ERR_INVALID
+    assert call([0, 1, 3], m=-1) == A.ALS_ERR_INVALID
+    assert call([0], m=0, nnz=0) == A.ALS_OK
 
 
 def test_version_string():

@@ -136,11 +136,11 @@ def test_jni_without_gpu_returns_null():
 
 @pytest.mark.gpu
 def test_jni_error_inside_dropin_returns_null():
-    """A CUDA-side failure raised inside doALSWithCSR (here: a rank the FP32
-    form does not take, f = 129) reaches the shim's catch block, which reports
-    it and returns null instead of letting the exception end the executor
-    process (reference CuMFJNIInterface.cpp:129-131). The CSR arrays the call
-    was given are freed on that path too."""
+    """A failure inside the half-step (here: a rank the FP32 form does not
+    take, f = 129) reaches the shim's catch block, which reports it and
+    returns null instead of letting the exception end the executor process
+    (reference CuMFJNIInterface.cpp:129-131). The Java arrays' critical
+    sections are released on that path too."""
     fk = _fake()
     f, n, m = 129, 3, 2
     th = np.arange(n * f, dtype=np.float32).reshape(n, f)
@@ -172,8 +172,8 @@ def test_jni_error_inside_dropin_returns_null():
 @pytest.mark.gpu
 def test_jni_kernel_timeout_returns_null():
     """A half-step whose kernel gives up a bounded wait (forced by the test
-    switch) makes doALSWithCSR throw instead of returning incomplete rows; the
-    Spark shim reports it and returns null, and the next call is correct."""
+    switch) fails instead of returning incomplete rows; the Spark shim reports
+    it and returns null, and the next call is correct."""
     fk = _fake()
     r = A.synth(A.scaled_config("ml1m", 0.1), seed=8)
     f = 32
