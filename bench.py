@@ -542,9 +542,26 @@ def run_engine(args):
         e2e_s = float(np.median(times[1:]))
         h2d = sum(a.nbytes for a in host) + 4 * (r.m + r.n) * f
         d2h = 4 * (r.m + r.n) * f
+        # the host link's rate for pinned host-to-device copies (three 512 MB
+        # copies after one untimed), the floor the e2e number is bound by
+        hb = torch.empty(1 << 29, dtype=torch.uint8).pin_memory()
+        db = torch.empty(1 << 29, dtype=torch.uint8, device=dev)
+        db.copy_(hb, non_blocking=True)
+        torch.cuda.synchronize(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(3):
+            db.copy_(hb, non_blocking=True)
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        h2d_gbs = 3 * hb.numel() / (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e9
+        del hb, db
         line["e2e"] = {"value": round(flop_iter / e2e_s / 1e9, 2), "unit": "GFLOP/s",
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "sec_per_iter": round(e2e_s, 4),
+                       "h2d_gbs_measured": round(h2d_gbs, 1),
+                       "h2d_floor_s": round(h2d / (h2d_gbs * 1e9), 4),
+                       "h2d_floor_frac": round(h2d / (h2d_gbs * 1e9) / e2e_s, 3),
                        "path": "als_half_step_host x2 (users, items), the Spark JNI entry's "
                                "half-step: CSR, theta and X in pinned host memory, the ratings "
                                "uploaded in row ranges overlapped with the solve of the previous "

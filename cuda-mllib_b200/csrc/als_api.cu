@@ -1171,7 +1171,7 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
 // path of the Spark JNI call, which uploads the three arrays into mallocBest
 // memory (CuMFJNIInterface.cpp:93-118) before doALSWithCSR uploads theta,
 // solves and downloads X, each transfer waiting for the one before. Here the
-// ratings cross PCIe in row ranges of about equal rating counts on a copy
+// ratings cross PCIe in row ranges by rating count on a copy
 // stream; each range is planned and solved on the caller's stream as soon as
 // it has landed, and its rows of X go back on a third stream while the next
 // range is solved. At the Netflix shape a side's ratings (0.8 GB) take about
@@ -1212,12 +1212,15 @@ struct HostPipe {
   }
 };
 
-// Row ranges [b[c], b[c + 1]) of about nnz / chunks ratings each (empty ranges
-// dropped); the row pointers are non-decreasing and end at nnz.
+// Row ranges [b[c], b[c + 1]) by rating count, the first and the last half
+// the size of the others: nothing can be solved before the first range has
+// landed, and the last range's solve and download follow the last upload, so
+// those two are the parts of the pipeline that do not overlap. Empty ranges
+// are dropped; the row pointers are non-decreasing and end at nnz.
 std::vector<int> host_ranges(const int *row_ptr, int m, long nnz, int chunks) {
   std::vector<int> b{0};
   for (int c = 1; c < chunks; ++c) {
-    const int target = (int)(nnz * c / chunks);
+    const int target = (int)(nnz * (2L * c - 1) / (2L * (chunks - 1)));
     const int r = (int)(std::lower_bound(row_ptr, row_ptr + m + 1, target) - row_ptr);
     if (r > b.back() && r < m) b.push_back(r);
   }
