@@ -559,6 +559,7 @@ def run_engine(args):
         line["e2e"] = {"value": round(flop_iter / e2e_s / 1e9, 2), "unit": "GFLOP/s",
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "sec_per_iter": round(e2e_s, 4),
+                       "ranks": 1,  # the host-buffer call runs on rank 0's GPU alone
                        "h2d_gbs_measured": round(h2d_gbs, 1),
                        "h2d_floor_s": round(h2d / (h2d_gbs * 1e9), 4),
                        "h2d_floor_frac": round(h2d / (h2d_gbs * 1e9) / e2e_s, 3),
