@@ -245,16 +245,19 @@ extern "C" jobjectArray Java_org_apache_spark_ml_recommendation_CuMFJNIInterface
     void *hc = J.GetPrimitiveArrayCritical(csrCol, nullptr);
     void *hv = J.GetPrimitiveArrayCritical(csrVal, nullptr);
     int rc = ALS_ERR_INVALID;
-    if (hr && hc && hv)
+    const char *why = "the JVM gave no access to the CSR arrays";
+    if (hr && hc && hv) {
       rc = als_half_step_host(stream.s, static_cast<const int *>(hr), static_cast<const int *>(hc),
                               static_cast<const float *>(hv), thetaTHost, XTHost, m, n, f, nnz,
                               (float)lambda, 0);
+      why = nullptr;
+    }
     if (hv) J.ReleasePrimitiveArrayCritical(csrVal, hv, 0);
     if (hc) J.ReleasePrimitiveArrayCritical(csrCol, hc, 0);
     if (hr) J.ReleasePrimitiveArrayCritical(csrRow, hr, 0);
     if (rc != ALS_OK)
       throw thrust::system_error(rc == ALS_ERR_INVALID ? cudaErrorInvalidValue : cudaErrorLaunchFailure,
-                                 thrust::cuda_category(), als_last_error());
+                                 thrust::cuda_category(), why ? why : als_last_error());
     // float[m][f], a frame of rows at a time
     jclass floatArrayClass = J.FindClass("[F");
     jobjectArray output = J.NewObjectArray(m, floatArrayClass, nullptr);
