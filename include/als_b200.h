@@ -210,8 +210,7 @@ int als_model_rmse(als_model *model, int64_t nt, const int32_t *d_u, const int32
 enum { ALS_ROW_EMPTY = 1, ALS_ROW_NOT_SPD = 2, ALS_ROW_REFINED_F64 = 4, ALS_ROW_CG_FALLBACK = 8 };
 
 /* Row sharding across GPUs, one process per GPU (no counterpart in the
- * reference, which runs one problem on one GPU per call; the survey's
- * multi-GPU design). Every rank holds the whole CSR/CSC and both factor
+ * reference, which runs one problem on one GPU per call). Every rank holds the whole CSR/CSC and both factor
  * matrices in its model, solves an nnz-balanced contiguous range of each
  * side's rows, and after each half-step the ranges are exchanged by one NCCL
  * all-gather (equal blocks of the largest range's row count; the other ranks'
