@@ -1180,7 +1180,14 @@ extern "C" void doALSWithCSR(cudaStream_t st, int *csrRowIndex, int *csrColIndex
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int kHostChunksMax = 16;
-constexpr long kHostChunkRatings = 12500000;  // automatic ranges: about this many ratings each
+// Automatic range counts. A side of short rows (more than one row per 1,000
+// ratings: the users side of the benchmark matrices) is bound by its solve,
+// and finer ranges hide more of the upload behind it (Netflix shape, users
+// half-step: 17.7 ms with 8 ranges, 17.1 with 12); a side of long rows is
+// bound by its upload, where more ranges only add their overhead (items
+// half-step: 18.9 ms with 8, 19.2 with 12).
+constexpr long kHostChunkRatings = 12500000;       // about this many ratings a range
+constexpr long kHostChunkRatingsShort = 8300000;   // the same for sides of short rows
 
 // The streams, events and workspace of one call. The destructor waits for all
 // three streams before the workspace goes back to the cache, on every path.
@@ -1246,10 +1253,11 @@ extern "C" int als_half_step_host(cudaStream_t st, const int *h_row_ptr, const i
   if (o.warm_start == ALS_WARM_PREVIOUS) o.warm_start = ALS_WARM_ZERO;  // no previous X here
   if (int rc = check_options(o, f); rc != ALS_OK) return rc;
   if (m == 0) return ALS_OK;
+  const bool short_rows = (long)m * 1000 > nnz;
+  const long per = short_rows ? kHostChunkRatingsShort : kHostChunkRatings;
   const int K = chunks ? chunks
-                       : (int)std::min<long>(kHostChunksMax / 2,
-                                             std::max<long>(1, (nnz + kHostChunkRatings - 1) /
-                                                                   kHostChunkRatings));
+                       : (int)std::min<long>(short_rows ? 12 : 8,
+                                             std::max<long>(1, (nnz + per - 1) / per));
   const std::vector<int> rb = host_ranges(h_row_ptr, m, nnz, K);
   const int nch = (int)rb.size() - 1;
   const int kind = lp_kind_of(o.precision);

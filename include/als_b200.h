@@ -144,8 +144,9 @@ int als_get_dropin_options(als_options *opt);
  * whole (CuMFJNIInterface.cpp:93-118 copies the three arrays into mallocBest
  * memory, then calls doALSWithCSR, als.cu:1001-1115), with the same inputs,
  * options (als_set_dropin_options) and result X, but pipelined: the ratings
- * are uploaded in `chunks` row ranges by rating count (0: one per ~12.5M
- * ratings, at most 8; the first and last range half the size of the others,
+ * are uploaded in `chunks` row ranges by rating count (0: chosen from nnz,
+ * at most 8, or 12 for sides of more than one row per 1,000 ratings, whose
+ * solve dominates; the first and last range half the size of the others,
  * since they do not overlap) on a copy stream, each range is solved on
  * `stream` as soon as it has landed, and its rows of X are downloaded while
  * the next range is solved. The arrays are the caller's and are not freed.
